@@ -1,0 +1,311 @@
+"""B200-native GTS: exact metric similarity search on a GPU pivot tree.
+
+Python host binding over the C ABI of ``libgts_b200.so`` (include/gts_b200.h).
+The compute path is the CUDA library; there is no CPU fallback -- importing
+works without a GPU, but every index operation needs the built library and a
+CUDA device and raises ``GtsError`` otherwise.
+
+The reference entry points are mirrored by name:
+
+=========================  =============================================
+reference (Source Code/GTS)  here
+=========================  =============================================
+``load`` file.cuh:28        :func:`load`
+``loadQuery`` file.cuh:112  :func:`load_queries`
+``loadUpdate`` update.cuh:43 :func:`load_updates`
+``indexConstru`` tree.cuh:332  :func:`indexConstru` / :class:`Index`
+``searchIndexKnnV2`` search_v2.cuh:975  :func:`searchIndexKnnV2` / :meth:`Index.knn`
+``searchIndexRnnV2`` search_v2.cuh:780  :func:`searchIndexRnnV2` / :meth:`Index.range`
+``updateIndexRnn`` update.cuh:449  :func:`updateIndexRnn` / :meth:`Index.update_run`
+``saveK`` / ``saveR`` file.cuh:154-199  :func:`saveK` / :func:`saveR`
+=========================  =============================================
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = ["GtsError", "Params", "Index", "load", "load_queries", "load_updates",
+           "indexConstru", "searchIndexKnnV2", "searchIndexRnnV2", "updateIndexRnn",
+           "saveK", "saveR", "lib_path", "FORM_PLAIN", "FORM_FAST"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libgts_b200.so")
+STR_STRIDE = 109
+FORM_PLAIN, FORM_FAST = 0, 1
+_lib = None
+
+
+class GtsError(RuntimeError):
+    """A GTS C-ABI call failed (message from gts_last_error)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"GTS error {code}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    """Runtime tunables; defaults are the reference's compile-time values
+    (tree.cuh:31-35, update.cuh:16)."""
+    _fields_ = [("tree_order", C.c_int), ("max_size", C.c_int), ("max_h", C.c_int),
+                ("dis_code", C.c_int), ("infi_dis", C.c_int), ("max_in_size", C.c_int),
+                ("mem_budget_gb", C.c_double)]
+
+    def __init__(self, tree_order=10, max_size=20, max_h=3, dis_code=100, infi_dis=10000,
+                 max_in_size=10, mem_budget_gb=0.0):
+        super().__init__(tree_order, max_size, max_h, dis_code, infi_dis, max_in_size,
+                         mem_budget_gb)
+
+
+class _Info(C.Structure):
+    _fields_ = [("num", C.c_int), ("dim", C.c_int), ("metric", C.c_int), ("tree_h", C.c_int),
+                ("max_node_num", C.c_int), ("tree_order", C.c_int), ("max_size", C.c_int),
+                ("device_bytes", C.c_size_t)]
+
+
+def lib_path() -> str:
+    return _LIB_PATH
+
+
+def _load_lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(
+            f"{_LIB_PATH} is not built; run `python -m gts_b200.build` (nvcc, sm_100a)")
+    lib = C.CDLL(_LIB_PATH)
+    lib.gts_last_error.restype = C.c_char_p
+    _lib = lib
+    return lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise GtsError(rc, _load_lib().gts_last_error().decode(errors="replace"))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+# --------------------------------------------------------------------- I/O
+
+def load(path: str):
+    """Reference text data file -> (dim, num, metric, rows | (strs, lens))."""
+    lib = _load_lib()
+    dim, num, metric = C.c_int(), C.c_int(), C.c_int()
+    rows, strs, lens = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    _check(lib.gts_load(path.encode(), C.byref(dim), C.byref(num), C.byref(metric),
+                        C.byref(rows), C.byref(strs), C.byref(lens)))
+    n, d, m = num.value, dim.value, metric.value
+    try:
+        if m == 6:
+            s = np.ctypeslib.as_array(C.cast(strs, C.POINTER(C.c_uint8)), (n, STR_STRIDE)).copy()
+            ln = np.ctypeslib.as_array(C.cast(lens, C.POINTER(C.c_int)), (n,)).copy()
+            return d, n, m, (s, ln)
+        r = np.ctypeslib.as_array(C.cast(rows, C.POINTER(C.c_float)), (n, d)).copy()
+        return d, n, m, r
+    finally:
+        for p in (rows, strs, lens):
+            if p.value:
+                lib.gts_free_host(p)
+
+
+def load_queries(path: str) -> np.ndarray:
+    lib = _load_lib()
+    q, n = C.c_void_p(), C.c_int()
+    _check(lib.gts_load_queries(path.encode(), C.byref(q), C.byref(n)))
+    try:
+        return np.ctypeslib.as_array(C.cast(q, C.POINTER(C.c_int)), (n.value,)).copy() \
+            if n.value else np.zeros(0, np.int32)
+    finally:
+        lib.gts_free_host(q)
+
+
+def load_updates(path: str):
+    lib = _load_lib()
+    f, i, n = C.c_void_p(), C.c_void_p(), C.c_int()
+    _check(lib.gts_load_updates(path.encode(), C.byref(f), C.byref(i), C.byref(n)))
+    try:
+        if n.value == 0:
+            return np.zeros(0, np.int32), np.zeros(0, np.int32)
+        return (np.ctypeslib.as_array(C.cast(f, C.POINTER(C.c_int)), (n.value,)).copy(),
+                np.ctypeslib.as_array(C.cast(i, C.POINTER(C.c_int)), (n.value,)).copy())
+    finally:
+        lib.gts_free_host(f)
+        lib.gts_free_host(i)
+
+
+def saveK(path_ids: str, path_dis: str, ids: np.ndarray, dists: np.ndarray) -> None:
+    """saveK layout (file.cuh:154-176): one line of k ids / k distances per query."""
+    with open(path_ids, "w") as fr, open(path_dis, "w") as fd:
+        for row_i, row_d in zip(ids, dists):
+            fr.write("".join(f"{int(v)} " for v in row_i) + "\n")
+            fd.write("".join(f"{float(v):f} " for v in row_d) + "\n")
+
+
+def saveR(path_ids: str, path_dis: str, ids, dists, counts, offsets) -> None:
+    """saveR layout (file.cuh:178-199): appended, one line per query."""
+    with open(path_ids, "a") as fr, open(path_dis, "a") as fd:
+        for c, o in zip(counts, offsets):
+            fr.write("".join(f"{int(v)} " for v in ids[o:o + c]) + "\n")
+            fd.write("".join(f"{float(v):f} " for v in dists[o:o + c]) + "\n")
+
+
+# --------------------------------------------------------------------- index
+
+class Index:
+    """A GTS pivot tree built and searched on the current CUDA device."""
+
+    def __init__(self, rows=None, metric: int = 2, strs=None, lens=None,
+                 params: Params | None = None, **param_kw):
+        lib = _load_lib()
+        self._lib = lib
+        self.params = params if params is not None else Params(**param_kw)
+        self._h = C.c_void_p()
+        if metric == 6:
+            strs = np.ascontiguousarray(strs, dtype=np.uint8)
+            lens = np.ascontiguousarray(lens, dtype=np.int32)
+            if strs.ndim != 2 or strs.shape[1] != STR_STRIDE:
+                raise ValueError(f"strs must be (num, {STR_STRIDE}) bytes")
+            _check(lib.gts_index_build(1, len(lens), 6, None, strs.ctypes.data_as(C.c_char_p),
+                                       _ip(lens), C.byref(self.params), C.byref(self._h)))
+        else:
+            rows = np.ascontiguousarray(rows, dtype=np.float32)
+            if rows.ndim != 2:
+                raise ValueError("rows must be (num, dim)")
+            _check(lib.gts_index_build(rows.shape[1], rows.shape[0], metric, _fp(rows), None, None,
+                                       C.byref(self.params), C.byref(self._h)))
+        self.metric = metric
+
+    @classmethod
+    def from_device(cls, d_rows_ptr: int, num: int, dim: int, metric: int = 2,
+                    params: Params | None = None, stream: int = 0, **param_kw):
+        self = cls.__new__(cls)
+        self._lib = _load_lib()
+        self.params = params if params is not None else Params(**param_kw)
+        self._h = C.c_void_p()
+        _check(self._lib.gts_index_build_device(dim, num, metric, C.c_void_p(d_rows_ptr), None, None,
+                                                C.byref(self.params), C.c_void_p(stream),
+                                                C.byref(self._h)))
+        self.metric = metric
+        return self
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.gts_index_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def info(self) -> dict:
+        i = _Info()
+        _check(self._lib.gts_index_info_get(self._h, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in _Info._fields_}
+
+    def export(self) -> dict:
+        inf = self.info
+        n, m = inf["num"], inf["max_node_num"]
+        out = {"id_list": np.empty(n, np.int32), "pid": np.empty(m, np.int32),
+               "min_dis": np.empty(m, np.float32), "size": np.empty(m, np.int32),
+               "lid": np.empty(m, np.int32), "is_leaf": np.empty(m, np.int32),
+               "exists": np.empty(m, np.int32)}
+        _check(self._lib.gts_index_export(self._h, _ip(out["id_list"]), _ip(out["pid"]),
+                                          _fp(out["min_dis"]), _ip(out["size"]), _ip(out["lid"]),
+                                          _ip(out["is_leaf"]), _ip(out["exists"])))
+        out["tree_h"] = inf["tree_h"]
+        return out
+
+    def set_stream(self, stream: int):
+        _check(self._lib.gts_index_set_stream(self._h, C.c_void_p(stream)))
+
+    def knn(self, qids, k: int, form: int = FORM_PLAIN, return_ids: bool = False):
+        q = np.ascontiguousarray(qids, dtype=np.int32)
+        kth = np.empty(len(q), np.float32)
+        ids = np.empty((len(q), k), np.int32) if return_ids else None
+        dis = np.empty((len(q), k), np.float32) if return_ids else None
+        _check(self._lib.gts_knn(self._h, _ip(q), len(q), k, form, _fp(kth),
+                                 _ip(ids) if return_ids else None,
+                                 _fp(dis) if return_ids else None))
+        return (kth, ids, dis) if return_ids else kth
+
+    def knn_device(self, d_qids: int, qnum: int, k: int, d_kth: int, d_ids: int = 0,
+                   d_dists: int = 0, form: int = FORM_PLAIN, stream: int = 0):
+        _check(self._lib.gts_knn_device(self._h, C.c_void_p(d_qids), qnum, k, form,
+                                        C.c_void_p(d_kth), C.c_void_p(d_ids or None),
+                                        C.c_void_p(d_dists or None), C.c_void_p(stream)))
+
+    def range(self, qids, r: float) -> np.ndarray:
+        q = np.ascontiguousarray(qids, dtype=np.int32)
+        out = np.empty(len(q), np.int32)
+        _check(self._lib.gts_range(self._h, _ip(q), len(q), C.c_float(r), _ip(out)))
+        return out
+
+    def range_device(self, d_qids: int, qnum: int, r: float, d_counts: int, stream: int = 0):
+        _check(self._lib.gts_range_device(self._h, C.c_void_p(d_qids), qnum, C.c_float(r),
+                                          C.c_void_p(d_counts), C.c_void_p(stream)))
+
+    def range_ids(self, qids, r: float, capacity: int | None = None):
+        """-> (counts, offsets, ids, dists); each query's hits in (distance, id) order."""
+        q = np.ascontiguousarray(qids, dtype=np.int32)
+        counts = np.empty(len(q), np.int32)
+        offs = np.empty(len(q), np.int32)
+        if capacity is None:
+            capacity = int(self.range(q, r).sum())
+        ids = np.empty(max(capacity, 1), np.int32)
+        dis = np.empty(max(capacity, 1), np.float32)
+        _check(self._lib.gts_range_ids(self._h, _ip(q), len(q), C.c_float(r), _ip(counts),
+                                       _ip(offs), _ip(ids), _fp(dis), C.c_size_t(capacity)))
+        tot = int(counts.sum())
+        return counts, offs, ids[:tot], dis[:tot]
+
+    def update_run(self, flags, ids, r: float):
+        """-> (counts per query op, search seconds, update seconds)."""
+        f = np.ascontiguousarray(flags, dtype=np.int32)
+        i = np.ascontiguousarray(ids, dtype=np.int32)
+        out = np.empty(max(1, int((f == 2).sum())), np.int32)
+        nq = C.c_int()
+        ts, tu = C.c_double(), C.c_double()
+        _check(self._lib.gts_update_run(self._h, _ip(f), _ip(i), len(f), C.c_float(r), _ip(out),
+                                        C.byref(nq), C.byref(ts), C.byref(tu)))
+        return out[:nq.value], ts.value, tu.value
+
+
+# ------------------------------------------------- reference-named wrappers
+
+def indexConstru(rows=None, metric: int = 2, strs=None, lens=None, **params) -> Index:
+    """indexConstru (tree.cuh:332): build the index."""
+    return Index(rows, metric, strs, lens, **params)
+
+
+def searchIndexKnnV2(index: Index, qids, k: int) -> np.ndarray:
+    """searchIndexKnnV2 (search_v2.cuh:975): -> res_dis, the k-th distance per query."""
+    return index.knn(qids, k)
+
+
+def searchIndexRnnV2(index: Index, qids, r: float) -> np.ndarray:
+    """searchIndexRnnV2 (search_v2.cuh:780): -> res, the result count per query."""
+    return index.range(qids, r)
+
+
+def updateIndexRnn(index: Index, flags, ids, r: float) -> np.ndarray:
+    """updateIndexRnn (update.cuh:449): -> the result count of every query op."""
+    return index.update_run(flags, ids, r)[0]

@@ -1,0 +1,48 @@
+// index.cuh -- the gts_index handle (host side) and internal entry points.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/gts_b200.h"
+#include "common.cuh"
+
+struct gts_index {
+    gts_params params;
+    int num = 0, dim = 0, metric = 0;
+    int tree_h = 0, max_node_num = 0;
+    cudaStream_t stream = 0;
+
+    float *rows = nullptr, *trows = nullptr;
+    char *strs = nullptr, *tstrs = nullptr;
+    int *lens = nullptr, *tlens = nullptr;
+    int *id_list = nullptr, *pos_of_id = nullptr;
+    int *node_pid = nullptr, *node_size = nullptr, *node_lid = nullptr, *node_pivot = nullptr;
+    float *node_min_dis = nullptr;
+    uint8_t *node_flags = nullptr;
+
+    // per-call scratch owned by the handle
+    int *d_counter = nullptr;   // persistent-kernel work counter
+    int *d_status = nullptr;    // kernel status word
+    size_t device_bytes = 0;
+
+    gts::DevTree dev() const;
+};
+
+namespace gts {
+
+// Build the tree for the data already placed in idx->rows / strs / lens.
+int build_tree(gts_index *idx, cudaStream_t s);
+// Free the tree arrays (not the data).
+void free_tree(gts_index *idx);
+void free_data(gts_index *idx);
+
+int search_knn(gts_index *idx, const int *d_qids, int qnum, int k, int form,
+               float *d_kth, int *d_ids, float *d_dists, cudaStream_t s);
+int search_range(gts_index *idx, const int *d_qids, int qnum, float r, int *d_counts,
+                 const uint32_t *d_deleted, cudaStream_t s);
+int search_range_ids(gts_index *idx, const int *d_qids, int qnum, float r, int *d_counts,
+                     int *d_ids, float *d_dists, const int *d_offsets, cudaStream_t s);
+
+template <typename T>
+int dev_alloc(T **p, size_t n, size_t *acct);
+
+}  // namespace gts

@@ -1,0 +1,157 @@
+/*
+ * gts_b200.h -- C ABI of the B200-native GTS similarity-search path.
+ *
+ * Plain C types only (pointers, sizes, an opaque handle, a cudaStream_t
+ * passed as void*).  Every function returns an int status (GTS_OK or a
+ * negative GTS_ERR_*); gts_last_error() gives the message of the last
+ * failure on the calling thread.  There is no global search state: all of it
+ * lives in the gts_index handle, so independent handles may be used from
+ * different threads.  One handle must not be used by two threads at once.
+ *
+ * Each entry point names the reference interface it replaces
+ * (paths inside the reference checkout: Source Code/GTS/...).
+ */
+#ifndef GTS_B200_H
+#define GTS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GTS_OK 0
+#define GTS_ERR_INVALID -1   /* bad argument (null pointer, k < 1, bad metric, size) */
+#define GTS_ERR_CUDA -2      /* CUDA runtime error or no usable device */
+#define GTS_ERR_NOMEM -3     /* device or host allocation failed / over budget */
+#define GTS_ERR_IO -4        /* file could not be opened or parsed */
+#define GTS_ERR_KERNEL -5    /* a kernel reported a bounded failure (status word) */
+
+#define GTS_STR_STRIDE 109   /* row stride of string objects (file.cuh:15) */
+
+/* Metric codes (data_info[2]; tree.cuh:81-154). */
+#define GTS_METRIC_LINF 0
+#define GTS_METRIC_L1 1
+#define GTS_METRIC_L2 2
+#define GTS_METRIC_ANGLE 5
+#define GTS_METRIC_EDIT 6
+
+/* Search forms. */
+#define GTS_FORM_PLAIN 0     /* traversal + FP32 filter + exact recheck */
+#define GTS_FORM_FAST 1      /* learned radius + BF16 tensor-core filter + exact recheck (L2) */
+
+typedef struct gts_index gts_index;
+
+/* Tunables.  The reference fixes these at compile time (tree.cuh:31-35,
+ * update.cuh:16; the argv overrides in src/main.cu:54-76 are commented out);
+ * here they are runtime values with the reference's defaults. */
+typedef struct {
+    int tree_order;      /* TREE_ORDER, default 10 */
+    int max_size;        /* MAX_SIZE,   default 20 */
+    int max_h;           /* MAX_H,      default 3 */
+    int dis_code;        /* DIS_CODE,   default 100 */
+    int infi_dis;        /* INFI_DIS,   default 10000 */
+    int max_in_size;     /* MAX_IN_SIZE (cache list), default 10 */
+    double mem_budget_gb;/* scratch budget per search call; 0 = 8 GB */
+} gts_params;
+
+typedef struct {
+    int num, dim, metric;
+    int tree_h, max_node_num;
+    int tree_order, max_size;
+    size_t device_bytes;  /* device memory held by the index */
+} gts_index_info;
+
+/* Fill *p with the reference defaults. */
+void gts_params_default(gts_params *p);
+
+const char *gts_last_error(void);
+
+/* ---------------------------------------------------------------- I/O */
+
+/* load (file.cuh:28-110): text data file, header "dim num metric".
+ * Allocates *rows (num*dim floats) or *strs (num*GTS_STR_STRIDE bytes) and
+ * *lens with malloc; free with gts_free_host. */
+int gts_load(const char *path, int *dim, int *num, int *metric,
+             float **rows, char **strs, int **lens);
+
+/* loadQuery (file.cuh:112-152): count line, then one id per line. */
+int gts_load_queries(const char *path, int **qids, int *qnum);
+
+/* loadUpdate (update.cuh:43-95): count line, then "flag id" per line. */
+int gts_load_updates(const char *path, int **flags, int **ids, int *nops);
+
+void gts_free_host(void *p);
+
+/* ---------------------------------------------------------------- index */
+
+/* indexConstru (tree.cuh:332-393): build the pivot tree on the device.
+ * Host inputs (copied to the device).  rows for metrics 0/1/2/5, strs+lens
+ * (num*GTS_STR_STRIDE bytes, lengths <= 108) for metric 6. */
+int gts_index_build(int dim, int num, int metric, const float *rows,
+                    const char *strs, const int *lens, const gts_params *params,
+                    gts_index **out);
+
+/* Same, with inputs already in device memory (not retained; copied). */
+int gts_index_build_device(int dim, int num, int metric, const float *d_rows,
+                           const char *d_strs, const int *d_lens,
+                           const gts_params *params, void *stream, gts_index **out);
+
+int gts_index_info_get(const gts_index *idx, gts_index_info *info);
+
+/* Copy the built tree to host buffers (each may be NULL): id_list[num];
+ * per node (max_node_num): pid, min_dis, size, lid, is_leaf, exists
+ * (exists = 1 where the reference's empty_list is 0). */
+int gts_index_export(const gts_index *idx, int *id_list, int *pid, float *min_dis,
+                     int *size, int *lid, int *is_leaf, int *exists);
+
+void gts_index_free(gts_index *idx);
+
+/* Set the stream used by the host-buffer entry points of this handle. */
+int gts_index_set_stream(gts_index *idx, void *stream);
+
+/* ---------------------------------------------------------------- search */
+
+/* searchIndexKnnV2 (search_v2.cuh:975-1228) -> res_dis.
+ * kth_out[q]: the k-th smallest distance of query object qids[q] (the query
+ * itself counts, at distance 0), INFI_DIS when fewer than k objects exist.
+ * ids_out / dists_out (qnum*k, nullable): the k nearest ids in ascending
+ * (distance, id) order.  Host buffers. */
+int gts_knn(gts_index *idx, const int *qids, int qnum, int k, int form,
+            float *kth_out, int *ids_out, float *dists_out);
+
+/* Same with device buffers, on `stream`. */
+int gts_knn_device(gts_index *idx, const int *d_qids, int qnum, int k, int form,
+                   float *d_kth, int *d_ids, float *d_dists, void *stream);
+
+/* searchIndexRnnV2 (search_v2.cuh:780-972) -> res.
+ * counts_out[q]: number of objects within r of qids[q] (itself included). */
+int gts_range(gts_index *idx, const int *qids, int qnum, float r, int *counts_out);
+
+int gts_range_device(gts_index *idx, const int *d_qids, int qnum, float r,
+                     int *d_counts, void *stream);
+
+/* saveR layout (file.cuh:178-199): ids of every object within r.
+ * counts_out[q] as above, offsets_out[q] = exclusive prefix of counts,
+ * ids_out/dists_out hold up to `capacity` entries grouped by query in
+ * ascending (distance, id) order.  Returns GTS_ERR_NOMEM (with counts and
+ * offsets filled) if the total exceeds capacity. */
+int gts_range_ids(gts_index *idx, const int *qids, int qnum, float r, int *counts_out,
+                  int *offsets_out, int *ids_out, float *dists_out, size_t capacity);
+
+/* ---------------------------------------------------------------- update */
+
+/* updateIndexRnn (update.cuh:449-638): replay a stream of operations
+ * (flag 0 insert, 1 delete, 2 range query of radius r) through the lazy
+ * cache list of params->max_in_size entries, rebuilding the index when the
+ * cache fills.  counts_out receives one entry per query op (*nq_out of
+ * them; size it to the number of flag-2 ops).  The index handle is updated
+ * in place (it holds the rebuilt tree afterwards). */
+int gts_update_run(gts_index *idx, const int *flags, const int *ids, int nops, float r,
+                   int *counts_out, int *nq_out, double *search_s, double *update_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GTS_B200_H */

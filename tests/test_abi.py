@@ -1,0 +1,98 @@
+"""The C-ABI library: it loads, exports every declared symbol, parses the
+reference file formats, and fails cleanly without a GPU (no compute here)."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import gts_b200 as gts
+from gts_b200 import datagen as G
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    syms = set()
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if not h.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(gts_[a-z0-9_]+)\s*\(", text):
+            syms.add(m.group(1))
+    return syms
+
+
+def test_library_exports_every_declared_symbol():
+    lib = gts.lib_path()
+    assert os.path.exists(lib), "libgts_b200.so is not built"
+    out = subprocess.run(["nm", "-D", "--defined-only", lib], capture_output=True, text=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    missing = _declared_symbols() - exported
+    assert not missing, f"declared but not exported: {sorted(missing)}"
+    C.CDLL(lib)   # and it loads
+
+
+def test_params_default_matches_reference():
+    lib = gts._load_lib()
+    p = gts.Params()
+    lib.gts_params_default(C.byref(p))
+    assert (p.tree_order, p.max_size, p.max_h, p.dis_code, p.infi_dis, p.max_in_size) == \
+        (10, 20, 3, 100, 10000, 10)
+
+
+def test_text_loaders_roundtrip(tmp_path):
+    rows = G.gmm_rows(50, 7, 3, 0.5, 1)
+    p = tmp_path / "d.txt"
+    G.write_data_text(str(p), 2, rows=rows)
+    d, n, m, r = gts.load(str(p))
+    assert (d, n, m) == (7, 50, 2)
+    np.testing.assert_allclose(r, rows, atol=1e-6)
+    strs, lens = G.word_strings(30, 2)
+    G.write_data_text(str(tmp_path / "s.txt"), 6, strs=strs, lens=lens)
+    d, n, m, (s2, l2) = gts.load(str(tmp_path / "s.txt"))
+    assert (n, m) == (30, 6)
+    np.testing.assert_array_equal(l2, lens)
+    np.testing.assert_array_equal(s2, strs)
+    G.write_queries(str(tmp_path / "q.txt"), [3, 1, 4])
+    assert gts.load_queries(str(tmp_path / "q.txt")).tolist() == [3, 1, 4]
+    G.write_updates(str(tmp_path / "u.txt"), [0, 1, 2], [5, 6, 7])
+    f, i = gts.load_updates(str(tmp_path / "u.txt"))
+    assert f.tolist() == [0, 1, 2] and i.tolist() == [5, 6, 7]
+
+
+def test_loader_errors(tmp_path):
+    with pytest.raises(gts.GtsError) as e:
+        gts.load(str(tmp_path / "missing.txt"))
+    assert e.value.code == -4
+    bad = tmp_path / "bad.txt"
+    bad.write_text("3 2 2\n1 2 3\n4 5\n")
+    with pytest.raises(gts.GtsError):
+        gts.load(str(bad))
+    long = tmp_path / "long.txt"
+    long.write_text("1 1 6\n" + "a" * 200 + "\n")
+    with pytest.raises(gts.GtsError):
+        gts.load(str(long))
+
+
+def test_reference_sample_parses():
+    from tests.golden_io import sample_dir
+    d = sample_dir()
+    if d is None:
+        pytest.skip("reference sample not present")
+    dim, n, m, rows = gts.load(os.path.join(d, "sbw_example.txt"))
+    assert (dim, n, m) == (300, 1000, 5)
+    metric, rows2 = G.read_text_rows(os.path.join(d, "sbw_example.txt"))
+    np.testing.assert_array_equal(rows, rows2)
+
+
+def test_no_device_is_a_clean_error():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(gts.GtsError) as e:
+        gts.Index(np.zeros((10, 4), np.float32), 2)
+    assert e.value.code == -2
