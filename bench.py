@@ -1,0 +1,333 @@
+"""Benchmark: exact kNN queries/s on one B200 (GTS similarity-search path).
+
+Workload (the headline configuration): 1,000,000 x 128 float32 vectors from a
+256-component Gaussian mixture (sigma 0.2, seeded, synthetic: the paper's
+data sets are not available), L2, 10,000 concurrent kNN queries with query
+ids drawn from the data, k = 8; GTS tree with TREE_ORDER 10, MAX_SIZE 20,
+MAX_H 6 (a perfect tree: 100,000 leaves of 10 objects).
+
+One step = one batch of 10,000 queries through the search.  The data set
+(512 MB) is larger than the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gts|reference]
+                    [--form fast|plain] [--k 8] [--queries 10000] [--n 1000000]
+
+--impl reference times the reference's own CUDA build (oracle/_ref, built
+from the reference sources) through its entry points on the same workload
+and prints the same JSON line with "impl": "reference".
+
+Multi-GPU (torchrun, one rank per GPU): every rank holds a replica of the
+index and answers its own 10,000 queries (weak scaling, no collective on the
+data path); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def workload(args, rank=0):
+    from gts_b200 import datagen as G
+    rows = G.gmm_rows(args.n, args.dim, 256, 0.2, seed=args.seed)
+    qids = G.query_ids(args.n, args.queries, seed=args.seed + 1 + 7919 * rank)
+    return rows, qids
+
+
+def config_dict(args, world):
+    return {"workload": f"gmm{args.n // 1000}k_d{args.dim}_l2_knn",
+            "n": args.n, "dim": args.dim, "metric": "L2", "queries_per_gpu": args.queries,
+            "k": args.k, "tree_order": 10, "max_size": 20, "max_h": args.max_h,
+            "form": args.form, "parallelism": f"query-sharded replicas x{world}",
+            "l2_flush": "no (512 MB data set > 126 MB L2)"}
+
+
+# ------------------------------------------------------------------ reference arm
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    drv = os.path.join(ROOT, "oracle", "_ref", "gts_ref_driver")
+    base = {"impl": "reference", "metric": "exact kNN queries/s", "unit": "queries/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "config": config_dict(args, 1)}
+    if not os.path.exists(drv):
+        print(json.dumps({**base, "unavailable": "reference CUDA build oracle/_ref/gts_ref_driver is not built"}))
+        return 0
+    from gts_b200 import datagen as G
+    rows, qids = workload(args)
+    with tempfile.TemporaryDirectory() as tmp:
+        dpath = os.path.join(tmp, "data.bin")
+        qpath = os.path.join(tmp, "q.txt")
+        G.write_data_bin(dpath, 2, rows)
+        G.write_queries(qpath, qids)
+        out = os.path.join(tmp, "res.txt")
+        cmd = [drv, dpath, qpath, "0", str(args.k), out, "--order", "10", "--max-size", "20",
+               "--max-h", str(args.max_h), "--budget-gb", "6",
+               "--repeat", str(args.warmup + args.steps)]
+        t0 = time.time()
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=3000)
+        wall = time.time() - t0
+        lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+        if p.returncode != 0 or not lines:
+            print(json.dumps({**base, "unavailable": f"reference run failed rc={p.returncode}: "
+                              f"{(p.stderr or p.stdout)[-300:]!r}"}))
+            return 0
+        info = json.loads(lines[-1])
+        runs = info["search_runs"][args.warmup:]
+        t = statistics.mean(runs)
+        value = args.queries / t
+        ref_kth = np.array([float(v) for v in open(out).read().split("\n")[2].split()], np.float32)
+    line = {**base, "value": value, "ms_per_step": t * 1e3, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian mixture)",
+            "build_s": info["build_s"], "wall_s": wall,
+            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": 1, "kind": "reference",
+                             "sample": f"reference CUDA build (searchIndexKnnV2) on the B200, "
+                                       f"{args.queries} queries per step, 6 GB list-table budget; "
+                                       f"one host thread drives it"},
+            "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    np.save(os.path.join(tempfile.gettempdir(), "gts_ref_kth.npy"), ref_kth)
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+
+def cpu_baseline(rows, qids, k, sample, kth_gpu):
+    """Exact multi-threaded brute force (reference leaf arithmetic) on the host."""
+    from oracle import oracle as O
+    ds = O.Dataset(2, rows)
+    q = qids[:sample]
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    kth, _, _ = O.knn_brute(ds, q, k, nthreads=cores)
+    dt = time.perf_counter() - t0
+    agree = int((kth == kth_gpu[:sample]).sum())
+    return {"value": len(q) / dt, "unit": "queries/s", "cores": cores, "kind": "port",
+            "sample": f"{len(q)} of the {len(qids)} queries, exact brute force over all "
+                      f"{len(rows)} rows in the reference's F64 leaf arithmetic, {cores} threads",
+            "agrees_with_gpu": f"{agree}/{len(q)}"}
+
+
+def run_gts(args):
+    import torch
+    import torch.distributed as dist
+
+    import gts_b200 as gts
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+
+    rows, qids = workload(args, rank)
+    d_rows = torch.from_numpy(rows).to(dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    idx = gts.Index.from_device(d_rows.data_ptr(), args.n, args.dim, 2, max_h=args.max_h,
+                                stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    del d_rows
+    form = gts.FORM_FAST if args.form == "fast" else gts.FORM_PLAIN
+    Q, k = args.queries, args.k
+    d_q = torch.from_numpy(qids).to(dev)
+    d_kth = torch.empty(Q, dtype=torch.float32, device=dev)
+
+    def step():
+        idx.knn_device(d_q.data_ptr(), Q, k, d_kth.data_ptr(), form=form, stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    stats = idx.search_stats()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for i in range(args.steps):
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    total_ms = t_start.elapsed_time(t_end)
+    per_launch_ms = [a.elapsed_time(b) for a, b in ev]
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    value = world * Q * args.steps / (total_ms / 1e3)
+    kth_gpu = d_kth.cpu().numpy()
+
+    # end to end through the host-buffer API: H2D of the query ids from pinned
+    # memory and D2H of the k-th distances inside every timed call
+    h_q = torch.from_numpy(qids).pin_memory().numpy()
+    for _ in range(max(1, args.warmup)):
+        idx.knn(h_q, k, form=form)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        kth_e2e = idx.knn(h_q, k, form=form)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * Q * args.steps / e2e_s, "unit": "queries/s",
+           "h2d_bytes_per_step": int(h_q.nbytes), "d2h_bytes_per_step": int(kth_e2e.nbytes)}
+    assert np.array_equal(kth_e2e, kth_gpu), "host-buffer and device-buffer paths disagree"
+
+    peak, peak_kind = measured_peaks()
+    d = args.dim
+    alg_bytes = 4 * d * (stats["objects"] + stats["pivots"]) + Q * (4 * d + 8 * k)
+    launch_ms = statistics.mean(per_launch_ms)
+    achieved = alg_bytes / (launch_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(f"{args.form}_k{k}_n{args.n}")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                "kernel": "k_search" if args.form == "plain" else "k_search (fast)",
+                "alg_bytes_per_launch": alg_bytes,
+                "per_query": {"leaf_objects": stats["objects"] / Q, "pivots": stats["pivots"] / Q,
+                              "exact_rechecks": stats["exact"] / Q}}
+    line = {"metric": "exact kNN queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Gaussian mixture; the paper's data sets are absent)",
+            "config": config_dict(args, world), "build_s": build_s, "roofline": roofline,
+            "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks.summary()}
+    if rank == 0 and world == 1 and args.cpu_sample > 0:
+        line["cpu_baseline"] = cpu_baseline(rows, qids, k, args.cpu_sample, kth_gpu)
+    if rank == 0:
+        print(json.dumps(line))
+    idx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["gts", "reference"], default="gts")
+    ap.add_argument("--form", choices=["fast", "plain"], default="plain")
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--dim", type=int, default=128)
+    ap.add_argument("--queries", type=int, default=10_000)
+    ap.add_argument("--k", type=int, default=8)
+    ap.add_argument("--max-h", type=int, default=6)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cpu-sample", type=int, default=256)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gts(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -237,6 +237,13 @@ class Index:
     def set_stream(self, stream: int):
         _check(self._lib.gts_index_set_stream(self._h, C.c_void_p(stream)))
 
+    def search_stats(self) -> dict:
+        """Work counters of the last search: leaf objects read, pivots
+        evaluated, exact recomputations, queries finished."""
+        out = (C.c_ulonglong * 4)()
+        _check(self._lib.gts_search_stats(self._h, out))
+        return {"objects": out[0], "pivots": out[1], "exact": out[2], "queries": out[3]}
+
     def knn(self, qids, k: int, form: int = FORM_PLAIN, return_ids: bool = False):
         q = np.ascontiguousarray(qids, dtype=np.int32)
         kth = np.empty(len(q), np.float32)

@@ -241,6 +241,8 @@ static int index_alloc_common(gts_index *idx)
     int rc;
     if ((rc = gts::dev_alloc(&idx->d_counter, 1, &acct)) != GTS_OK) return rc;
     if ((rc = gts::dev_alloc(&idx->d_status, 1, &acct)) != GTS_OK) return rc;
+    if ((rc = gts::dev_alloc(&idx->d_stats, 4, &acct)) != GTS_OK) return rc;
+    cudaMemset(idx->d_stats, 0, 4 * sizeof(unsigned long long));
     idx->device_bytes += acct;
     return GTS_OK;
 }
@@ -375,7 +377,18 @@ extern "C" void gts_index_free(gts_index *idx)
     gts::free_data(idx);
     if (idx->d_counter) cudaFree(idx->d_counter);
     if (idx->d_status) cudaFree(idx->d_status);
+    if (idx->d_stats) cudaFree(idx->d_stats);
     delete idx;
+}
+
+extern "C" int gts_search_stats(const gts_index *idx, unsigned long long *out4)
+{
+    if (!idx || !out4) {
+        gts_set_error("null argument");
+        return GTS_ERR_INVALID;
+    }
+    GTS_CUDA_TRY(cudaMemcpy(out4, idx->d_stats, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    return GTS_OK;
 }
 
 extern "C" int gts_index_set_stream(gts_index *idx, void *stream)

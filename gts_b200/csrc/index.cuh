@@ -22,6 +22,7 @@ struct gts_index {
     // per-call scratch owned by the handle
     int *d_counter = nullptr;   // persistent-kernel work counter
     int *d_status = nullptr;    // kernel status word
+    unsigned long long *d_stats = nullptr;   // work counters of the last search
     size_t device_bytes = 0;
 
     gts::DevTree dev() const;

@@ -32,18 +32,17 @@ constexpr int kStrStride = 109;   // reference string row stride (file.cuh:15)
 // ---------------------------------------------------------------------------
 
 // Sequential F64-accumulated distance.  `pow(float_diff, 2)` in the
-// reference resolves to a double-returning overload equal to the exact
-// square, so the fused multiply-add below adds the same value.
+// reference resolves to a double-returning overload that is not always the
+// exact square (measured on the device: ~6% of inputs differ in the last
+// bit), and `pow(x, 0.5)` is not always `sqrt(x)`; both are called here
+// literally so every value matches the reference bit for bit.
 __device__ __forceinline__ double dist_row_f64(const float *__restrict__ a,
                                                const float *__restrict__ b,
                                                int dim, int metric)
 {
     double r = 0.0;
     if (metric == kL2) {
-        for (int j = 0; j < dim; j++) {
-            double x = (double)(a[j] - b[j]);
-            r = fma(x, x, r);
-        }
+        for (int j = 0; j < dim; j++) r += pow(a[j] - b[j], 2);
         return pow(r, 0.5);
     } else if (metric == kL1) {
         for (int j = 0; j < dim; j++) r += abs(a[j] - b[j]);
@@ -70,17 +69,14 @@ __device__ __forceinline__ double dist_row_f64(const float *__restrict__ a,
 }
 
 // Sequential F32-accumulated distance (`float result += pow(..)` adds in
-// double and rounds to float at every step).
+// double and rounds to float at every step), same literal calls.
 __device__ __forceinline__ float dist_row_f32(const float *__restrict__ a,
                                               const float *__restrict__ b,
                                               int dim, int metric)
 {
     float r = 0.f;
     if (metric == kL2) {
-        for (int j = 0; j < dim; j++) {
-            double x = (double)(a[j] - b[j]);
-            r = (float)fma(x, x, (double)r);
-        }
+        for (int j = 0; j < dim; j++) r += pow(a[j] - b[j], 2);
         r = pow(r, 0.5);
         return r;
     } else if (metric == kL1) {

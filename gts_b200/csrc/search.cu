@@ -63,6 +63,7 @@ struct SearchArgs {
     const uint32_t *deleted;
     int *counter;
     int *status;
+    unsigned long long *stats;   // [objects filtered, pivots evaluated, exact values, queries]
     float rel_eps;   // relative pruning slack
     float abs_eps;   // absolute pruning slack
 };
@@ -86,6 +87,7 @@ struct __align__(16) SearchSmem {
     int cpos[kLeafObjCap];     // positions needing an exact value
     int nint, nleaf, ncpos;
     int top, ncand, q, qid, cnt, overflow;
+    unsigned long long n_obj, n_piv, n_exact;
     double R;
 };
 
@@ -253,6 +255,7 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
             s.ncand = 0;
             s.cnt = 0;
             s.overflow = 0;
+            s.n_obj = s.n_piv = s.n_exact = 0;
             s.R = knn ? DBL_MAX : (double)a.r;
         }
         if (t.metric == kEdit) {
@@ -309,6 +312,8 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
                 s.nint = nint;
                 s.nleaf = nleaf;
                 s.ncpos = 0;
+                s.n_obj += nobj;
+                s.n_piv += nint;
             }
             __syncthreads();
             const int nint = s.nint, nleaf = s.nleaf;
@@ -358,6 +363,7 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
                 __syncthreads();
                 // exact values for the collected positions
                 const int ncpos = s.ncpos;
+                if (tid == 0) s.n_exact += ncpos;
                 if (knn && s.ncand + ncpos > kCandCap) compact_candidates(s, a.k);
                 for (int c = tid; c < ncpos; c += kThreads) {
                     int pos = s.cpos[c];
@@ -446,7 +452,15 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
         } else if (tid == 0) {
             if (a.mode == kModeRangeCount) a.counts[q] = s.cnt;
         }
-        if (tid == 0 && s.overflow) atomicMax(a.status, (int)kKsStackOverflow);
+        if (tid == 0) {
+            if (s.overflow) atomicMax(a.status, (int)kKsStackOverflow);
+            if (a.stats) {
+                atomicAdd(&a.stats[0], s.n_obj);
+                atomicAdd(&a.stats[1], s.n_piv);
+                atomicAdd(&a.stats[2], s.n_exact);
+                atomicAdd(&a.stats[3], 1ull);
+            }
+        }
         __syncthreads();
     }
 }
@@ -458,6 +472,7 @@ static int run_search(gts_index *idx, SearchArgs &a, cudaStream_t st)
     if (a.qnum <= 0) return GTS_OK;
     a.t = idx->dev();
     a.counter = idx->d_counter;
+    a.stats = idx->d_stats;
     a.status = idx->d_status;
     if (idx->metric == kAngle) {
         a.rel_eps = 1e-5f;
@@ -475,6 +490,7 @@ static int run_search(gts_index *idx, SearchArgs &a, cudaStream_t st)
     }
     GTS_CUDA_TRY(cudaMemsetAsync(idx->d_counter, 0, sizeof(int), st));
     GTS_CUDA_TRY(cudaMemsetAsync(idx->d_status, 0, sizeof(int), st));
+    GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, 4 * sizeof(unsigned long long), st));
     size_t smem = sizeof(SearchSmem);
     GTS_CUDA_TRY(cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int dev = 0, nsm = 148, per_sm = 1;

@@ -110,6 +110,12 @@ void gts_index_free(gts_index *idx);
 /* Set the stream used by the host-buffer entry points of this handle. */
 int gts_index_set_stream(gts_index *idx, void *stream);
 
+/* Work counters of the last search call on this handle (no reference
+ * counterpart; the reference prints only wall-clock times, main.cu:106-109):
+ * out4[0] objects whose rows were read at leaves, out4[1] pivots evaluated,
+ * out4[2] exact (reference-order) recomputations, out4[3] queries finished. */
+int gts_search_stats(const gts_index *idx, unsigned long long *out4);
+
 /* ---------------------------------------------------------------- search */
 
 /* searchIndexKnnV2 (search_v2.cuh:975-1228) -> res_dis.

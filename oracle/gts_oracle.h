@@ -90,10 +90,14 @@ int orc_range_brute(const orc_data *d, const int *qids, int qnum, float r,
 
 /* Stream update (update.cuh:449-638).  flags/ids: the update file's ops.
  * counts_out receives one entry per query op (flag 2); *nq_out their number.
- * The data set is copied internally; `d` is not modified. */
+ * The data set is copied internally; `d` is not modified.
+ * exact == 0: the reference's v1 tree search restated (it skips last-level
+ *             nodes above MAX_SIZE, so it undercounts on non-perfect trees);
+ * exact != 0: the tree part of each count is a brute-force scan of the live
+ *             rows (the exact answer), everything else unchanged. */
 int orc_update_run(const orc_data *d, const orc_params *p, int max_in_size,
                    const int *flags, const int *ids, int nops, float r,
-                   int *counts_out, int *nq_out);
+                   int exact, int *counts_out, int *nq_out);
 
 #ifdef __cplusplus
 }

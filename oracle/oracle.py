@@ -152,13 +152,15 @@ def range_brute(ds, qids, r: float, nthreads: int = 0) -> np.ndarray:
     return out
 
 
-def update_run(ds, p, max_in_size: int, flags, ids, r: float) -> np.ndarray:
+def update_run(ds, p, max_in_size: int, flags, ids, r: float, exact: bool = False) -> np.ndarray:
+    """Counts per query op; exact=True scans live rows instead of the
+    reference's v1 tree search (which skips oversized last-level nodes)."""
     f = np.ascontiguousarray(flags, dtype=np.int32)
     i = np.ascontiguousarray(ids, dtype=np.int32)
     out = np.empty(int((f == 2).sum()) + 1, dtype=np.int32)
     nq = C.c_int(0)
     rc = lib().orc_update_run(ds.ref, C.byref(p), max_in_size, _iptr(f), _iptr(i), len(f),
-                              C.c_float(r), _iptr(out), C.byref(nq))
+                              C.c_float(r), 1 if exact else 0, _iptr(out), C.byref(nq))
     if rc != 0:
         raise RuntimeError(f"orc_update_run failed: {rc}")
     return out[:nq.value]

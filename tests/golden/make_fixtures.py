@@ -146,8 +146,14 @@ def gen_case(name, c, driver, tmp, out):
     print(f"{name}: ok ({', '.join(k for k in res if k.startswith(('knn', 'range', 'update_c')))})")
 
 
-def gen_sample(gts_bin, sample_dir, out):
-    """Unmodified reference CLI on the reference's sample data (README.md:49-84)."""
+def gen_sample(driver, sample_dir, out):
+    """The reference on its own sample data (README.md:49-84), text files read
+    by its own loader, default tree parameters (MAX_H 3).
+
+    The unmodified CLI (src/main.cu) cannot run on a 180 GB B200: it sizes its
+    list table as half the free memory in an int count of elements
+    (search_v2.cuh:995-1001), which overflows, and stops with "out of memory".
+    The harness runs the same entry points with a 6 GB list-table budget."""
     data = os.path.join(sample_dir, "sbw_example.txt")
     qid = os.path.join(sample_dir, "sbw_example_qid.txt")
     upd = os.path.join(sample_dir, "sbw_example_u.txt")
@@ -157,9 +163,7 @@ def gen_sample(gts_bin, sample_dir, out):
             "sample_update_r59.txt": [data, upd, "2", "59"]}
     for fname, args in runs.items():
         dst = os.path.join(out, fname)
-        p = subprocess.run([gts_bin, *args, dst], capture_output=True, text=True)
-        if p.returncode != 0:
-            raise RuntimeError(f"GTS {args} failed: {p.stderr[-1000:]}")
+        run([driver, *args, dst, "--max-h", "3", "--budget-gb", "6"])
         print(f"{fname}: ok")
 
 
@@ -174,10 +178,10 @@ def main():
     driver = os.path.join(a.ref, "gts_ref_driver")
     tmp = tempfile.mkdtemp(prefix="gts_golden_")
     try:
-        for name in a.cases.split(","):
+        for name in [c for c in a.cases.split(",") if c and c != "none"]:
             gen_case(name, CASES[name], driver, tmp, a.out)
         if a.sample:
-            gen_sample(os.path.join(a.ref, "GTS"), a.sample, a.out)
+            gen_sample(driver, a.sample, a.out)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
 

@@ -58,7 +58,12 @@ def test_tree_equals_oracle(oracle, metric, n, dim, max_h):
     np.testing.assert_array_equal(e["exists"].astype(bool), ex)
     for key in ("pid", "size", "lid", "is_leaf"):
         np.testing.assert_array_equal(e[key][ex], getattr(t, key)[ex], err_msg=key)
-    np.testing.assert_array_equal(e["min_dis"][ex], t.min_dis[ex])
+    if metric == 5:
+        # angle goes through acosf, whose last bit differs between the host
+        # library and the device (the device value is the reference's)
+        np.testing.assert_array_max_ulp(e["min_dis"][ex], t.min_dis[ex], maxulp=4)
+    else:
+        np.testing.assert_array_equal(e["min_dis"][ex], t.min_dis[ex])
 
 
 @pytest.mark.parametrize("metric,n,dim,max_h", SHAPES)
@@ -110,7 +115,9 @@ def test_update_equals_oracle(oracle):
     flags, ids = G.update_stream(1500, 400, seed=12, max_in_size=10)
     r = float(np.float32(G.quantile_radius(2, 0.01, 30000, 13, rows=rows)))
     p = oracle.params(max_h=3)
-    want = oracle.update_run(ds, p, 10, flags, ids, r)
+    # 1500 rows drift to sizes whose last-level nodes exceed MAX_SIZE after
+    # rebuilds; the reference skips those, the exact count does not
+    want = oracle.update_run(ds, p, 10, flags, ids, r, exact=True)
     with gts.Index(rows, 2, max_h=3, max_in_size=10) as idx:
         got, ts, tu = idx.update_run(flags, ids, r)
     np.testing.assert_array_equal(got, want)
