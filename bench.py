@@ -40,13 +40,19 @@ sys.path.insert(0, ROOT)
 HBM_FALLBACK_GBS = 6650.0
 
 
-def measured_peaks():
+BF16_FALLBACK_TFLOPS = 1590.0
+
+
+def measured_peaks_all():
+    """Roofline denominators: the driver-measured copy bandwidth and burst bf16
+    GEMM throughput of this pool's B200s, else the pool's earlier figures."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
-    return HBM_FALLBACK_GBS, "fallback"
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]),
+                "kind": "measured"}
+    return {"hbm_gbs": HBM_FALLBACK_GBS, "bf16_tflops": BF16_FALLBACK_TFLOPS, "kind": "fallback"}
 
 
 class ClockSampler:
@@ -274,28 +280,49 @@ def run_gts(args):
            "h2d_bytes_per_step": int(h_q.nbytes), "d2h_bytes_per_step": int(kth_e2e.nbytes)}
     assert np.array_equal(kth_e2e, kth_gpu), "host-buffer and device-buffer paths disagree"
 
-    peak, peak_kind = measured_peaks()
+    peaks = measured_peaks_all()
     d = args.dim
-    alg_bytes = 4 * d * (stats["objects"] + stats["pivots"]) + Q * (4 * d + 8 * k)
+    # this library's kernels per step (CUB's radix-sort kernels not counted):
+    # plain: k_search; fast: k_fast_keys, k_fast_init, 2 x k_fast_tile,
+    # k_add_stat, k_fast_final, and k_search + 3 helpers when queries fall back
+    launches_per_step = 1 if args.form == "plain" else 6 + (4 if stats["fallback"] else 0)
     launch_ms = statistics.mean(per_launch_ms)
-    achieved = alg_bytes / (launch_ms / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
             traffic = json.load(f).get(f"{args.form}_k{k}_n{args.n}")
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                "kernel": "k_search" if args.form == "plain" else "k_search (fast)",
-                "alg_bytes_per_launch": alg_bytes,
-                "per_query": {"leaf_objects": stats["objects"] / Q, "pivots": stats["pivots"] / Q,
-                              "exact_rechecks": stats["exact"] / Q}}
+    if args.form == "plain":
+        # every leaf row and pivot row a query reads, plus its own row and result
+        alg_bytes = 4 * d * (stats["objects"] + stats["pivots"]) + Q * (4 * d + 8 * k)
+        achieved = alg_bytes / (launch_ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                    "peak_kind": peaks["kind"], "kernel": "k_search",
+                    "alg_bytes_per_launch": alg_bytes,
+                    "per_query": {"leaf_objects": stats["objects"] / Q, "pivots": stats["pivots"] / Q,
+                                  "exact_rechecks": stats["exact"] / Q}}
+    else:
+        # tensor pipe: every streamed block is one 128 x 144 x Kp MMA chain for
+        # the BF16 high part and one for the low part of the queries
+        kp = (d + 63) // 64 * 64
+        flops = stats["blocks"] * 2 * 128 * 144 * kp * 2
+        achieved = flops / (launch_ms / 1e3) / 1e12
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
+                    "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"], "traffic": traffic,
+                    "peak_kind": peaks["kind"], "kernel": "k_fast_tile",
+                    "mma_flops_per_launch": flops,
+                    "streamed_bytes_per_launch": stats["bytes"],
+                    "streamed_gbs": stats["bytes"] / (launch_ms / 1e3) / 1e9,
+                    "per_query": {"blocks": stats["blocks"] / Q, "appended": stats["appended"] / Q,
+                                  "exact_rechecks": stats["exact"] / Q,
+                                  "fallback_queries": stats["fallback"], "passes": stats["passes"]}}
     line = {"metric": "exact kNN queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Gaussian mixture; the paper's data sets are absent)",
             "config": config_dict(args, world), "build_s": build_s, "roofline": roofline,
-            "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks.summary()}
+            "e2e": e2e, "gpu_launches": args.steps * launches_per_step, "clocks": clocks.summary()}
     if rank == 0 and world == 1 and args.cpu_sample > 0:
         line["cpu_baseline"] = cpu_baseline(rows, qids, k, args.cpu_sample, kth_gpu)
     if rank == 0:

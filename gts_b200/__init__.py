@@ -240,9 +240,12 @@ class Index:
     def search_stats(self) -> dict:
         """Work counters of the last search: leaf objects read, pivots
         evaluated, exact recomputations, queries finished."""
-        out = (C.c_ulonglong * 4)()
+        out = (C.c_ulonglong * 8)()
         _check(self._lib.gts_search_stats(self._h, out))
-        return {"objects": out[0], "pivots": out[1], "exact": out[2], "queries": out[3]}
+        return {"objects": out[0], "pivots": out[1], "exact": out[2], "queries": out[3],
+                "fallback": out[4], "appended": out[5], "passes": out[6],
+                # fast form: [0] counts operand blocks and [1] their bytes
+                "blocks": out[0], "bytes": out[1]}
 
     def knn(self, qids, k: int, form: int = FORM_PLAIN, return_ids: bool = False):
         q = np.ascontiguousarray(qids, dtype=np.int32)

@@ -8,12 +8,14 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libgts_b200.so")
+CLI = os.path.join(HERE, "gts")
+CLI_SRC = os.path.join(HERE, "csrc", "cli.cpp")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
 def sources():
     return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")) +
-                  glob.glob(os.path.join(HERE, "csrc", "*.cpp")))
+                  [p for p in glob.glob(os.path.join(HERE, "csrc", "*.cpp")) if p != CLI_SRC])
 
 
 def headers():
@@ -22,10 +24,18 @@ def headers():
 
 
 def up_to_date() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(CLI):
         return False
-    t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(f) <= t for f in sources() + headers())
+    t = min(os.path.getmtime(LIB), os.path.getmtime(CLI))
+    return all(os.path.getmtime(f) <= t for f in sources() + headers() + [CLI_SRC])
+
+
+def build_cli() -> str:
+    """The GTS command line (drop-in for the reference's bin/GTS)."""
+    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(HERE, "..", "include"), CLI_SRC,
+           "-L", HERE, "-lgts_b200", "-Wl,-rpath,$ORIGIN", "-o", CLI]
+    subprocess.run(cmd, check=True)
+    return CLI
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
@@ -48,6 +58,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             raise RuntimeError(f"nvcc failed on {src}")
     cmd = ["nvcc", "-shared", *ARCH, "-o", LIB, *objs, "-lcudart"]
     subprocess.run(cmd, check=True)
+    build_cli()
     return LIB
 
 

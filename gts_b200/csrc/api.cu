@@ -241,8 +241,8 @@ static int index_alloc_common(gts_index *idx)
     int rc;
     if ((rc = gts::dev_alloc(&idx->d_counter, 1, &acct)) != GTS_OK) return rc;
     if ((rc = gts::dev_alloc(&idx->d_status, 1, &acct)) != GTS_OK) return rc;
-    if ((rc = gts::dev_alloc(&idx->d_stats, 4, &acct)) != GTS_OK) return rc;
-    cudaMemset(idx->d_stats, 0, 4 * sizeof(unsigned long long));
+    if ((rc = gts::dev_alloc(&idx->d_stats, gts::kStatsN, &acct)) != GTS_OK) return rc;
+    cudaMemset(idx->d_stats, 0, gts::kStatsN * sizeof(unsigned long long));
     idx->device_bytes += acct;
     return GTS_OK;
 }
@@ -378,16 +378,17 @@ extern "C" void gts_index_free(gts_index *idx)
     if (idx->d_counter) cudaFree(idx->d_counter);
     if (idx->d_status) cudaFree(idx->d_status);
     if (idx->d_stats) cudaFree(idx->d_stats);
+    if (idx->scratch) cudaFree(idx->scratch);
     delete idx;
 }
 
-extern "C" int gts_search_stats(const gts_index *idx, unsigned long long *out4)
+extern "C" int gts_search_stats(const gts_index *idx, unsigned long long *out8)
 {
-    if (!idx || !out4) {
+    if (!idx || !out8) {
         gts_set_error("null argument");
         return GTS_ERR_INVALID;
     }
-    GTS_CUDA_TRY(cudaMemcpy(out4, idx->d_stats, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    GTS_CUDA_TRY(cudaMemcpy(out8, idx->d_stats, gts::kStatsN * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
     return GTS_OK;
 }
 

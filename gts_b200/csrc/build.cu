@@ -203,8 +203,27 @@ static inline unsigned grid_for(size_t n, int block, unsigned cap = 148u * 32u)
     return (unsigned)(g > cap ? cap : g);
 }
 
+int ensure_scratch(gts_index *idx, size_t bytes)
+{
+    if (idx->scratch_bytes >= bytes) return GTS_OK;
+    if (idx->scratch) cudaFree(idx->scratch);
+    idx->scratch = nullptr;
+    idx->scratch_bytes = 0;
+    if (cudaMalloc(&idx->scratch, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        idx->scratch = nullptr;
+        gts_set_error("cudaMalloc of %zu bytes of search scratch failed", bytes);
+        return GTS_ERR_NOMEM;
+    }
+    idx->scratch_bytes = bytes;
+    return GTS_OK;
+}
+
 void free_tree(gts_index *idx)
 {
+    if (idx->fast_recs) cudaFree(idx->fast_recs);
+    idx->fast_recs = nullptr;
+    idx->fast_nb = 0;
     void *ps[] = {idx->trows, idx->tstrs, idx->tlens, idx->id_list, idx->pos_of_id, idx->node_pid,
                   idx->node_size, idx->node_lid, idx->node_pivot, idx->node_min_dis,
                   idx->node_flags};

@@ -22,13 +22,31 @@ struct gts_index {
     // per-call scratch owned by the handle
     int *d_counter = nullptr;   // persistent-kernel work counter
     int *d_status = nullptr;    // kernel status word
-    unsigned long long *d_stats = nullptr;   // work counters of the last search
+    unsigned long long *d_stats = nullptr;   // work counters of the last search (kStatsN)
+    bool keep_stats = false;                 // a nested search adds to, not resets, the counters
     size_t device_bytes = 0;
+
+    // tensor-core filter (L2): per-block operand records, built on first use
+    unsigned char *fast_recs = nullptr;
+    int fast_nb = 0;
+    int last_fast_overflow = 0;
+
+    // reusable per-call scratch (grown on demand, freed with the handle)
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
 
     gts::DevTree dev() const;
 };
 
 namespace gts {
+
+// Search work counters (gts_search_stats):
+//   [0] plain: leaf objects read          fast: operand blocks streamed
+//   [1] plain: pivots evaluated           fast: bytes streamed
+//   [2] exact (reference-order) values    [3] plain: queries finished
+//   [4] fast: queries answered again on the plain path
+//   [5] fast: candidates appended         [6] fast: filter passes
+constexpr int kStatsN = 8;
 
 // Build the tree for the data already placed in idx->rows / strs / lens.
 int build_tree(gts_index *idx, cudaStream_t s);
@@ -45,5 +63,30 @@ int search_range_ids(gts_index *idx, const int *d_qids, int qnum, float r, int *
 
 template <typename T>
 int dev_alloc(T **p, size_t n, size_t *acct);
+
+// Grow idx->scratch to at least `bytes`.
+int ensure_scratch(gts_index *idx, size_t bytes);
+
+bool fast_supported(const gts_index *idx, int k);
+int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
+                    float *d_dists, cudaStream_t s);
+
+// A set of device allocations freed together on scope exit.
+struct DevVec {
+    void *ps[8] = {};
+    int n = 0;
+    ~DevVec()
+    {
+        for (int i = 0; i < n; i++)
+            if (ps[i]) cudaFree(ps[i]);
+    }
+    template <typename T>
+    int alloc(T **p, size_t cnt)
+    {
+        int rc = dev_alloc(p, cnt, nullptr);
+        if (rc == 0 && n < 8) ps[n++] = *p;
+        return rc;
+    }
+};
 
 }  // namespace gts

@@ -490,7 +490,7 @@ static int run_search(gts_index *idx, SearchArgs &a, cudaStream_t st)
     }
     GTS_CUDA_TRY(cudaMemsetAsync(idx->d_counter, 0, sizeof(int), st));
     GTS_CUDA_TRY(cudaMemsetAsync(idx->d_status, 0, sizeof(int), st));
-    GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, 4 * sizeof(unsigned long long), st));
+    if (!idx->keep_stats) GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, kStatsN * sizeof(unsigned long long), st));
     size_t smem = sizeof(SearchSmem);
     GTS_CUDA_TRY(cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int dev = 0, nsm = 148, per_sm = 1;
@@ -516,11 +516,12 @@ static int run_search(gts_index *idx, SearchArgs &a, cudaStream_t st)
 int search_knn(gts_index *idx, const int *d_qids, int qnum, int k, int form, float *d_kth, int *d_ids,
                float *d_dists, cudaStream_t st)
 {
-    (void)form;
     if (k < 1 || k > kMaxK) {
         gts_set_error("k must be in [1, %d], got %d", kMaxK, k);
         return GTS_ERR_INVALID;
     }
+    if (form == 1 && qnum > 0 && fast_supported(idx, k))
+        return search_knn_fast(idx, d_qids, qnum, k, d_kth, d_ids, d_dists, st);
     SearchArgs a{};
     a.qids = d_qids;
     a.qnum = qnum;

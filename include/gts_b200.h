@@ -111,10 +111,15 @@ void gts_index_free(gts_index *idx);
 int gts_index_set_stream(gts_index *idx, void *stream);
 
 /* Work counters of the last search call on this handle (no reference
- * counterpart; the reference prints only wall-clock times, main.cu:106-109):
- * out4[0] objects whose rows were read at leaves, out4[1] pivots evaluated,
- * out4[2] exact (reference-order) recomputations, out4[3] queries finished. */
-int gts_search_stats(const gts_index *idx, unsigned long long *out4);
+ * counterpart; the reference prints only wall-clock times, main.cu:106-109).
+ * out8[0] plain form: leaf objects read; fast form: operand blocks streamed
+ * out8[1] plain form: pivots evaluated;  fast form: bytes streamed
+ * out8[2] exact (reference-order) recomputations
+ * out8[3] queries finished by the plain traversal
+ * out8[4] fast form: queries answered again on the plain path
+ * out8[5] fast form: candidates appended
+ * out8[6] fast form: filter passes over the blocks; out8[7] reserved */
+int gts_search_stats(const gts_index *idx, unsigned long long *out8);
 
 /* ---------------------------------------------------------------- search */
 

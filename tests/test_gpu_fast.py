@@ -1,0 +1,55 @@
+"""The fast form (BF16 tensor-core filter + exact recheck): bit-identical
+answers to exact brute force in the reference's leaf arithmetic."""
+import numpy as np
+import pytest
+
+import gts_b200 as gts
+from gts_b200 import datagen as G
+
+pytestmark = pytest.mark.gpu
+
+CASES = [  # (n, dim, comps, sigma, nq, max_h)
+    (20000, 128, 32, 0.2, 300, 5),     # the headline shape, small
+    (9000, 64, 16, 0.3, 257, 4),       # ragged query count, n not a multiple of 128
+    (7777, 100, 8, 0.25, 130, 4),      # dimension padded to 128 inside the filter
+    (4000, 32, 4, 1.0, 129, 4),
+    (3000, 128, 1, 0.05, 64, 4),       # one tight cluster: many near-ties
+]
+
+
+@pytest.mark.parametrize("n,dim,comps,sigma,nq,max_h", CASES)
+def test_fast_knn_equals_brute_force(oracle, n, dim, comps, sigma, nq, max_h):
+    rows = G.gmm_rows(n, dim, comps, sigma, seed=n + dim)
+    ds = oracle.Dataset(2, rows)
+    q = G.query_ids(n, nq, seed=n + 1)
+    with gts.Index(rows, 2, max_h=max_h) as idx:
+        for k in (1, 8, 33, 64):
+            kth, ids, dis = idx.knn(q, k, form=gts.FORM_FAST, return_ids=True)
+            bk, bi, bd = oracle.knn_brute(ds, q, k)
+            np.testing.assert_array_equal(ids, bi, err_msg=f"k={k}")
+            np.testing.assert_array_equal(kth, bk, err_msg=f"k={k}")
+            np.testing.assert_array_equal(dis, bd, err_msg=f"k={k}")
+
+
+def test_fast_equals_plain_and_counts_work():
+    rows = G.gmm_rows(30000, 128, 64, 0.2, seed=5)
+    q = G.query_ids(30000, 1000, seed=6)
+    with gts.Index(rows, 2, max_h=5) as idx:
+        a = idx.knn(q, 8, form=gts.FORM_PLAIN, return_ids=True)
+        b = idx.knn(q, 8, form=gts.FORM_FAST, return_ids=True)
+        st = idx.search_stats()
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+    assert st["objects"] > 0 and st["exact"] >= 8 * len(q)
+
+
+def test_fast_falls_back_outside_its_shape(oracle):
+    """Dimensions above the filter's limit and k above 64 take the plain path."""
+    rows = G.gmm_rows(3000, 200, 8, 0.3, seed=7)
+    ds = oracle.Dataset(2, rows)
+    q = G.query_ids(3000, 40, seed=8)
+    with gts.Index(rows, 2, max_h=4) as idx:
+        kth = idx.knn(q, 8, form=gts.FORM_FAST)
+        np.testing.assert_array_equal(kth, oracle.knn_brute(ds, q, 8)[0])
+        kth = idx.knn(q, 100, form=gts.FORM_FAST)
+        np.testing.assert_array_equal(kth, oracle.knn_brute(ds, q, 100)[0])
