@@ -123,7 +123,10 @@ def config_dict(args, world):
     return {"workload": f"gmm{args.n // 1000}k_d{args.dim}_l2_knn",
             "n": args.n, "dim": args.dim, "metric": "L2", "queries_per_gpu": args.queries,
             "k": args.k, "tree_order": 10, "max_size": 20, "max_h": args.max_h,
-            "form": args.form, "parallelism": f"query-sharded replicas x{world}",
+            "form": args.form + ("" if args.form == "plain" else
+                                 (" (bf16 filter, two passes)" if args.no_learn else
+                                  " (learned radius + bf16 filter)")),
+            "parallelism": f"query-sharded replicas x{world}",
             "l2_flush": "no (512 MB data set > 126 MB L2)"}
 
 
@@ -223,6 +226,16 @@ def run_gts(args):
     build_s = time.perf_counter() - t0
     del d_rows
     form = gts.FORM_FAST if args.form == "fast" else gts.FORM_PLAIN
+    learn = None
+    if args.form == "fast" and not args.no_learn:
+        # learned radius: 200,000 exact radii from the index itself, trained on
+        # the device before the timed region
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        learn = idx.learn_radius(n_train=args.train, k_max=64, epochs=12, seed=args.seed)
+        torch.cuda.synchronize()
+        learn["train_s"] = time.perf_counter() - t0
+        learn["n_train"] = args.train
     Q, k = args.queries, args.k
     d_q = torch.from_numpy(qids).to(dev)
     d_kth = torch.empty(Q, dtype=torch.float32, device=dev)
@@ -321,7 +334,8 @@ def run_gts(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Gaussian mixture; the paper's data sets are absent)",
-            "config": config_dict(args, world), "build_s": build_s, "roofline": roofline,
+            "config": config_dict(args, world), "build_s": build_s, "learned_radius": learn,
+            "roofline": roofline,
             "e2e": e2e, "gpu_launches": args.steps * launches_per_step, "clocks": clocks.summary()}
     if rank == 0 and world == 1 and args.cpu_sample > 0:
         line["cpu_baseline"] = cpu_baseline(rows, qids, k, args.cpu_sample, kth_gpu)
@@ -340,7 +354,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["gts", "reference"], default="gts")
-    ap.add_argument("--form", choices=["fast", "plain"], default="plain")
+    ap.add_argument("--form", choices=["fast", "plain"], default="fast")
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--dim", type=int, default=128)
     ap.add_argument("--queries", type=int, default=10_000)
@@ -348,6 +362,9 @@ def main():
     ap.add_argument("--max-h", type=int, default=6)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-sample", type=int, default=256)
+    ap.add_argument("--no-learn", action="store_true",
+                    help="fast form without the learned radius (two filter passes)")
+    ap.add_argument("--train", type=int, default=200_000, help="learned-radius training samples")
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

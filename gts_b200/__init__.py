@@ -35,7 +35,21 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libgts_b200.so")
 STR_STRIDE = 109
 FORM_PLAIN, FORM_FAST = 0, 1
+RADIUS_MODEL_PARAMS = 128 * 33 + 128 + 128 * 128 + 128 + 128 + 1
 _lib = None
+
+
+def radius_model_grad(X, target, params, norm):
+    """(loss, grad) of the radius model on a batch, from the device kernels."""
+    X = np.ascontiguousarray(X, np.float32)
+    t = np.ascontiguousarray(target, np.float32)
+    P = np.ascontiguousarray(params, np.float32)
+    nm = np.ascontiguousarray(norm, np.float32)
+    g = np.empty(RADIUS_MODEL_PARAMS, np.float32)
+    loss = C.c_float()
+    _check(_load_lib().gts_radius_model_grad(_fp(X), _fp(t), len(t), _fp(P), _fp(nm), _fp(g),
+                                             C.byref(loss)))
+    return loss.value, g
 
 
 class GtsError(RuntimeError):
@@ -286,6 +300,22 @@ class Index:
                                        _ip(offs), _ip(ids), _fp(dis), C.c_size_t(capacity)))
         tot = int(counts.sum())
         return counts, offs, ids[:tot], dis[:tot]
+
+    def learn_radius(self, n_train: int = 200_000, k_max: int = 64, epochs: int = 12,
+                     seed: int = 0) -> dict:
+        """Train the learned kNN radius (GTS_FORM_FAST then starts from it)."""
+        rmse, widen = C.c_float(), C.c_float()
+        _check(self._lib.gts_learn_radius(self._h, n_train, k_max, epochs, C.c_uint(seed),
+                                          C.byref(rmse), C.byref(widen)))
+        return {"val_rmse_log": rmse.value, "widen": widen.value}
+
+    def radius_model(self) -> dict:
+        P = np.empty(RADIUS_MODEL_PARAMS, np.float32)
+        norm = np.empty(66, np.float32)
+        extra = np.empty(3, np.float32)
+        _check(self._lib.gts_radius_model_params(self._h, _fp(P), _fp(norm), _fp(extra)))
+        return {"params": P, "norm": norm, "ymu": float(extra[0]), "ysig": float(extra[1]),
+                "widen": float(extra[2])}
 
     def update_run(self, flags, ids, r: float):
         """-> (counts per query op, search seconds, update seconds)."""

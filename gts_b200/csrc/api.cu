@@ -379,6 +379,9 @@ extern "C" void gts_index_free(gts_index *idx)
     if (idx->d_status) cudaFree(idx->d_status);
     if (idx->d_stats) cudaFree(idx->d_stats);
     if (idx->scratch) cudaFree(idx->scratch);
+    if (idx->mlp_P) cudaFree(idx->mlp_P);
+    if (idx->mlp_norm) cudaFree(idx->mlp_norm);
+    if (idx->mlp_piv) cudaFree(idx->mlp_piv);
     delete idx;
 }
 

@@ -43,7 +43,7 @@ constexpr int kFN = 144;              // B rows per block: objects + centre rows
 constexpr int kFT = 128;              // queries per tile (A rows, TMEM lanes)
 constexpr int kFMaxKp = 128;          // padded dimension limit of this path (shared-memory budget)
 constexpr int kFMaxK = 64;
-constexpr int kFCand = 1024;          // candidate slots per query
+constexpr int kFCand = 2048;          // candidate slots per query
 constexpr long long kFWait = 1ll << 24;   // bounded mbarrier polls
 
 // Filter error-bound constants (see header comment).
@@ -144,79 +144,72 @@ struct FastTileArgs {
     int *cand_pos;              // [qnum][kFCand]
     float *cand_lb;             // [qnum][kFCand]
     int *cand_cnt;              // [qnum]
-    int *r2_bits;               // [qnum] radius^2 bound as int bits: read as the seed, tightened by atomicMin
-    int append;                 // 0: only tighten the bound; 1: also append candidates
+    int *r2_bits;               // [qnum] radius^2 bound as int bits (the append pass's seed)
+    float *hbuf;                // bound pass: [qnum][splits][CG][k] smallest upper bounds
+    int *item_counter;          // persistent-CTA work queue over (tile, split) items
+    int ntiles;
     int *status;
     unsigned long long *stats;
 };
 
+constexpr int kFS = 3;   // B stages: copies run two blocks ahead of the MMAs
+
 struct __align__(8) FastCtl {
-    uint64_t full[2];
+    uint64_t full[kFS];
     uint64_t mmad[2];
     uint32_t tmem;
-    int nown;
+    int item;
     int err;
-    int pend[2];   // copies issued per stage
-    int done[2];   // copy completions observed per stage (by the MMA issuer)
-    int seq[4];    // block of step i at seq[i & 3], written two steps ahead
+    int pend[kFS];     // copies issued per stage
+    int done[kFS];     // copy completions observed per stage (by the MMA issuer)
     int qis[kFT];      // query index of each TMEM lane
     float q2s[kFT];    // |q|^2 (from FP64)
     float qns[kFT];    // |q|
-    int gen_i;     // generator: next own-list index
-    int gen_b;     // generator: next stream block
-    int gen_o;     // generator: own-list cursor for skipping
-    int own[kFT];
 };
 
-// Block order of one CTA: first the distinct blocks holding its queries (a
-// tight running radius early), then every block b = split (mod splits) that
-// is not one of those.  Each block reaches a CTA's bound heap at most once --
-// a repeated object would count twice among the k smallest and make the
-// running radius too small.  Called by thread 0 only, once per step.
-__device__ __forceinline__ int fast_gen_next(FastCtl &c, int splits)
-{
-    if (c.gen_i < c.nown) return c.own[c.gen_i++];
-    for (;;) {
-        int b = c.gen_b;
-        c.gen_b += splits;
-        while (c.gen_o < c.nown && c.own[c.gen_o] < b) c.gen_o++;
-        if (c.gen_o < c.nown && c.own[c.gen_o] == b) continue;
-        return b;
-    }
-}
-
-// CG column groups of 4 warps: warps w, w+4, ... share TMEM lanes 32*(w%4)..+31
-// (the same 32 queries) and split the 128 object columns, so an SM runs
-// 4*CG warps of epilogue.  Each thread keeps its own k smallest upper bounds;
-// the per-query bound of the CTA is the k-th smallest of their union.
-template <int CG>
+// Persistent filter kernel, one CTA per SM.  Work items are (tile, split):
+// the 128 queries of a tile (sorted by tree position) against the blocks
+// b = split (mod splits).  MODE 0: bound pass -- every thread keeps its
+// k smallest upper bounds and writes them to hbuf; MODE 2: the same while
+// also appending objects within the running bound capped by a seed (one
+// pass for a seeded run); MODE 1: append pass --
+// objects whose lower bound is within the query's seed are appended.
+//
+// CG column groups of 4 warps: warps w, w+4, ... share TMEM lanes
+// 32*(w%4)..+31 (the same 32 queries) and split the 128 object columns, so an
+// SM runs 4*CG warps of epilogue.
+//
+// Pipeline per CTA (global block counter gi, barrier parities follow it):
+// bulk copy of block gi into B[gi % 3] -> MMA chain into D[gi % 2] (TMEM
+// columns 0 / 256) -> epilogue on D[gi % 2].  The MMA of block gi+1 is
+// issued before the epilogue of block gi; the copy of block gi+3 after it.
+template <int CG, int MODE>
 __global__ void __launch_bounds__(128 * CG, 1) k_fast_tile(FastTileArgs a)
 {
     constexpr int NT = 128 * CG;
     constexpr int CW = 128 / CG;   // object columns per thread
     extern __shared__ __align__(1024) unsigned char fsm[];
-    // 1024-aligned carve-up: A_hi | A_lo | B0 | B1 | heap | ctl
+    // 1024-aligned carve-up: A_hi | A_lo | B0 | B1 | B2 | heap | ctl
     unsigned char *base = (unsigned char *)(((uintptr_t)fsm + 1023) & ~(uintptr_t)1023);
     const FastShape fs = a.fs;
     unsigned char *A_hi = base;
     unsigned char *A_lo = A_hi + fs.atile_bytes;
     const uint32_t rec_pad = (fs.rec_bytes + 1023u) & ~1023u;
-    unsigned char *Bs[2] = {A_lo + fs.atile_bytes, A_lo + fs.atile_bytes + rec_pad};
-    float *heap = reinterpret_cast<float *>(Bs[1] + rec_pad);
-    FastCtl &ctl = *reinterpret_cast<FastCtl *>(heap + NT * a.k);
+    unsigned char *B0 = A_lo + fs.atile_bytes;
+    float *heap = reinterpret_cast<float *>(B0 + kFS * rec_pad);
+    FastCtl &ctl = *reinterpret_cast<FastCtl *>(heap + (MODE == 1 ? 0 : NT * a.k));
 
     const int t = threadIdx.x, warp = t >> 5;
     const int lq = t & 127, g = t >> 7;   // query lane, column group
-    const int tile = blockIdx.x, split = blockIdx.y;
-    const int k = a.k;
+    const int k = a.k, splits = a.splits;
 
     if (t == 0) {
-        for (int s = 0; s < 2; s++) {
+        for (int s = 0; s < kFS; s++) {
             mbar_init(&ctl.full[s], 1);
-            mbar_init(&ctl.mmad[s], 1);
             ctl.pend[s] = 0;
             ctl.done[s] = 0;
         }
+        for (int s = 0; s < 2; s++) mbar_init(&ctl.mmad[s], 1);
         ctl.err = 0;
         fence_mbar_init();
     }
@@ -224,214 +217,226 @@ __global__ void __launch_bounds__(128 * CG, 1) k_fast_tile(FastTileArgs a)
         tmem_alloc(&ctl.tmem, 512);
         tmem_relinquish();
     }
-
-    // ---- A operand (first column group): the query, split into BF16 hi + lo
-    if (g == 0) {
-        const int slot = tile * kFT + lq;
-        const int qi = slot < a.qnum ? a.order[slot] : -1;
-        const int qid = qi >= 0 ? a.qids[qi] : -1;
-        const float *row = qid >= 0 ? a.rows + (size_t)qid * a.dim : nullptr;
-        double acc = 0.0;
-        for (int j0 = 0; j0 < fs.kp; j0 += 8) {
-            unsigned short hi[8], lo[8];
-#pragma unroll
-            for (int u = 0; u < 8; u++) {
-                int j = j0 + u;
-                float x = (row && j < a.dim) ? row[j] : 0.f;
-                acc += (double)x * x;
-                hi[u] = f2bf(x);
-                lo[u] = f2bf(x - bf2f(hi[u]));
-            }
-            uint4 vh, vl;
-            vh.x = hi[0] | ((uint32_t)hi[1] << 16); vh.y = hi[2] | ((uint32_t)hi[3] << 16);
-            vh.z = hi[4] | ((uint32_t)hi[5] << 16); vh.w = hi[6] | ((uint32_t)hi[7] << 16);
-            vl.x = lo[0] | ((uint32_t)lo[1] << 16); vl.y = lo[2] | ((uint32_t)lo[3] << 16);
-            vl.z = lo[4] | ((uint32_t)lo[5] << 16); vl.w = lo[6] | ((uint32_t)lo[7] << 16);
-            uint32_t off = sw128_offset(lq, j0, kFT);
-            *reinterpret_cast<uint4 *>(A_hi + off) = vh;
-            *reinterpret_cast<uint4 *>(A_lo + off) = vl;
-        }
-        ctl.qis[lq] = qi;
-        ctl.q2s[lq] = (float)acc;
-        ctl.qns[lq] = (float)sqrt(acc);
-        ctl.own[lq] = qid >= 0 ? a.pos_of_id[qid] / kFB : 0x7fffffff;
-    }
-    for (int i = 0; i < k; i++) heap[i * NT + t] = FLT_MAX;
-    fence_proxy_async_smem();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (t == 0) {   // distinct own blocks (queries are sorted by position)
-        int n = 0;
-        for (int i = 0; i < kFT; i++) {
-            int b = ctl.own[i];
-            if (b == 0x7fffffff) break;
-            if (n == 0 || ctl.own[n - 1] != b) ctl.own[n++] = b;
-        }
-        ctl.nown = n;
-        int own_here = 0;   // own blocks that also belong to this CTA's stream
-        for (int i = 0; i < n; i++) own_here += (ctl.own[i] % a.splits) == split;
-        ctl.gen_i = 0;
-        ctl.gen_b = split;
-        ctl.gen_o = 0;
-        ctl.seq[0] = own_here;   // handed to every thread below
-    }
-    __syncthreads();
     const uint32_t tmem = ctl.tmem;
-    const int qi = ctl.qis[lq];
-    const float q2 = ctl.q2s[lq], qn = ctl.qns[lq];
-    const int nstream = (a.nb - split + a.splits - 1) / a.splits;
-    const int nseq = ctl.nown + (nstream > 0 ? nstream : 0) - ctl.seq[0];
-    __syncthreads();   // every thread has read seq[0] before the generator reuses it
     const uint32_t idesc = idesc_bf16_f32(kFT, kFN);
     const uint32_t a_hi_s = smem_u32(A_hi), a_lo_s = smem_u32(A_lo);
+    long long gblk = 0;   // blocks this CTA has run through the pipeline
+    unsigned long long blocks_done = 0, appended = 0;
 
-    auto issue_copy = [&](int i) {
-        int s = i & 1;
-        const int blk = fast_gen_next(ctl, a.splits);
-        ctl.seq[i & 3] = blk;
-        const unsigned char *src = a.recs + (size_t)blk * fs.rec_bytes;
-        mbar_arrive_expect_tx(&ctl.full[s], fs.rec_bytes);
-        bulk_g2s(Bs[s], src, fs.rec_bytes, &ctl.full[s]);
-        ctl.pend[s]++;
-    };
-    auto issue_mma = [&](int i) -> bool {
-        int s = i & 1;
-        if (!mbar_wait(&ctl.full[s], (i >> 1) & 1, kFWait)) return false;
-        ctl.done[s]++;
-        tc_fence_after();
-        const uint32_t b_s = smem_u32(Bs[s]);
-        const uint32_t d = tmem + (uint32_t)(s * 256);
-        const int ksteps = fs.kp / 16;
-        for (int kk = 0; kk < ksteps; kk++) {
-            uint32_t off = (uint32_t)(kk >> 2) * (kFT * 128u) + (uint32_t)(kk & 3) * 32u;
-            uint32_t boff = (uint32_t)(kk >> 2) * (kFN * 128u) + (uint32_t)(kk & 3) * 32u;
-            mma_bf16(d, smem_desc_sw128(a_hi_s + off, 1024), smem_desc_sw128(b_s + boff, 1024), idesc,
-                     kk > 0 ? 1u : 0u);
-        }
-        for (int kk = 0; kk < ksteps; kk++) {
-            uint32_t off = (uint32_t)(kk >> 2) * (kFT * 128u) + (uint32_t)(kk & 3) * 32u;
-            uint32_t boff = (uint32_t)(kk >> 2) * (kFN * 128u) + (uint32_t)(kk & 3) * 32u;
-            mma_bf16(d, smem_desc_sw128(a_lo_s + off, 1024), smem_desc_sw128(b_s + boff, 1024), idesc, 1u);
-        }
-        mma_commit(&ctl.mmad[s]);
-        return true;
-    };
-
-    if (t == 0) {
-        for (int i = 0; i < 2 && i < nseq; i++) issue_copy(i);
-        if (nseq > 0 && !issue_mma(0)) ctl.err = 1;
-    }
-    __syncthreads();
-
-    const float seed = qi >= 0 ? __int_as_float(a.r2_bits[qi]) : FLT_MAX;   // FLT_MAX: no seed
-    float R2 = seed;
-    unsigned long long appended = 0;
-    int hidx = 0;
-    const float cq = 2.f * kKappa * qn;
-    unsigned long long blocks_done = 0;
-    for (int i = 0; i < nseq; i++) {
-        const int s = i & 1;
-        if (t == 0 && !ctl.err && i + 1 < nseq) {
-            if (!issue_mma(i + 1)) ctl.err = 2;
-        }
-        if (!mbar_wait(&ctl.mmad[s], (i >> 1) & 1, kFWait)) ctl.err = 3;
-        tc_fence_after();
+    for (;;) {
+        if (t == 0) ctl.item = atomicAdd(a.item_counter, 1);
         __syncthreads();
-        if (ctl.err) break;
-        mbar_wait(&ctl.full[s], (i >> 1) & 1, kFWait);   // make the record's tail visible to every thread
-        const int blk = ctl.seq[i & 3];
-        const float *o2 = reinterpret_cast<const float *>(Bs[s] + fs.btile_bytes);
-        const float *rn = o2 + 128;
-        const float cn = o2[256];
-        const int nvalid = reinterpret_cast<const int *>(o2)[257];
-        const uint32_t taddr = tmem + ((uint32_t)(warp & 3) * 32u << 16) + (uint32_t)(s * 256);
-        float v[16];
-        tmem_ld16(taddr + 128, v);
-        const float qc = v[0] + v[1] + v[2];
-        const float ec = 2.f * kEpsC * qn * cn + 1e-6f;
-        // lb = (|q|^2 - 2 q.c - ec - 2e-6 |q|^2) + |o|^2 (1 - 2e-6) - cq |r| - 2 q.r
-        const float t0 = q2 - 2.f * qc - ec - 2e-6f * q2;
-#pragma unroll 1
-        for (int c = g * CW; c < (g + 1) * CW; c += 16) {
-            tmem_ld16(taddr + (uint32_t)c, v);
-            if (qi < 0) continue;
+        const int item = ctl.item;
+        if (item >= a.ntiles * splits || ctl.err) break;
+        const int tile = item / splits, split = item % splits;
+
+        // ---- A operand (first column group): the query, split into BF16 hi + lo
+        if (g == 0) {
+            const int slot = tile * kFT + lq;
+            const int qi = slot < a.qnum ? a.order[slot] : -1;
+            const int qid = qi >= 0 ? a.qids[qi] : -1;
+            const float *row = qid >= 0 ? a.rows + (size_t)qid * a.dim : nullptr;
+            double acc = 0.0;
+            for (int j0 = 0; j0 < fs.kp; j0 += 8) {
+                unsigned short hi[8], lo[8];
 #pragma unroll
-            for (int u = 0; u < 16; u++) {
-                const int j = c + u;
-                if (j >= nvalid) break;
-                const float oo = o2[j], rr = rn[j];
-                const float lb = fmaf(-2.f, v[u], fmaf(-cq, rr, fmaf(oo, 0.999998f, t0)));
-                if (lb <= R2) {
-                    if (a.append) {
-                        const int pos = blk * kFB + j;
-                        int sl = atomicAdd(&a.cand_cnt[qi], 1);
-                        if (sl < kFCand) {
-                            a.cand_pos[(size_t)qi * kFCand + sl] = pos;
-                            a.cand_lb[(size_t)qi * kFCand + sl] = lb;
+                for (int u = 0; u < 8; u++) {
+                    int j = j0 + u;
+                    float x = (row && j < a.dim) ? row[j] : 0.f;
+                    acc += (double)x * x;
+                    hi[u] = f2bf(x);
+                    lo[u] = f2bf(x - bf2f(hi[u]));
+                }
+                uint4 vh, vl;
+                vh.x = hi[0] | ((uint32_t)hi[1] << 16); vh.y = hi[2] | ((uint32_t)hi[3] << 16);
+                vh.z = hi[4] | ((uint32_t)hi[5] << 16); vh.w = hi[6] | ((uint32_t)hi[7] << 16);
+                vl.x = lo[0] | ((uint32_t)lo[1] << 16); vl.y = lo[2] | ((uint32_t)lo[3] << 16);
+                vl.z = lo[4] | ((uint32_t)lo[5] << 16); vl.w = lo[6] | ((uint32_t)lo[7] << 16);
+                uint32_t off = sw128_offset(lq, j0, kFT);
+                *reinterpret_cast<uint4 *>(A_hi + off) = vh;
+                *reinterpret_cast<uint4 *>(A_lo + off) = vl;
+            }
+            ctl.qis[lq] = qi;
+            ctl.q2s[lq] = (float)acc;
+            ctl.qns[lq] = (float)sqrt(acc);
+        }
+        if (MODE != 1)
+            for (int i = 0; i < k; i++) heap[i * NT + t] = FLT_MAX;
+        fence_proxy_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        const int qi = ctl.qis[lq];
+        const float q2 = ctl.q2s[lq], qn = ctl.qns[lq];
+        const float cq = 2.f * kKappa * qn;
+        const float seed = (MODE != 0 && qi >= 0) ? __int_as_float(a.r2_bits[qi]) : FLT_MAX;
+        float R2 = seed;
+        int hidx = 0;
+        const int n = (a.nb - split + splits - 1) / splits;   // blocks of this item
+
+        auto issue_copy = [&](int j) {
+            const long long gi = gblk + j;
+            const int s = (int)(gi % kFS);
+            const unsigned char *src = a.recs + (size_t)(split + (size_t)j * splits) * fs.rec_bytes;
+            mbar_arrive_expect_tx(&ctl.full[s], fs.rec_bytes);
+            bulk_g2s(B0 + (size_t)s * rec_pad, src, fs.rec_bytes, &ctl.full[s]);
+            ctl.pend[s]++;
+        };
+        auto issue_mma = [&](int j) -> bool {
+            const long long gi = gblk + j;
+            const int s = (int)(gi % kFS), d = (int)(gi & 1);
+            if (!mbar_wait(&ctl.full[s], (uint32_t)((gi / kFS) & 1), kFWait)) return false;
+            ctl.done[s]++;
+            tc_fence_after();
+            const uint32_t b_s = smem_u32(B0 + (size_t)s * rec_pad);
+            const uint32_t dt = tmem + (uint32_t)(d * 256);
+            const int ksteps = fs.kp / 16;
+            for (int kk = 0; kk < ksteps; kk++) {
+                uint32_t off = (uint32_t)(kk >> 2) * (kFT * 128u) + (uint32_t)(kk & 3) * 32u;
+                uint32_t boff = (uint32_t)(kk >> 2) * (kFN * 128u) + (uint32_t)(kk & 3) * 32u;
+                mma_bf16(dt, smem_desc_sw128(a_hi_s + off, 1024), smem_desc_sw128(b_s + boff, 1024), idesc,
+                         kk > 0 ? 1u : 0u);
+            }
+            for (int kk = 0; kk < ksteps; kk++) {
+                uint32_t off = (uint32_t)(kk >> 2) * (kFT * 128u) + (uint32_t)(kk & 3) * 32u;
+                uint32_t boff = (uint32_t)(kk >> 2) * (kFN * 128u) + (uint32_t)(kk & 3) * 32u;
+                mma_bf16(dt, smem_desc_sw128(a_lo_s + off, 1024), smem_desc_sw128(b_s + boff, 1024), idesc, 1u);
+            }
+            mma_commit(&ctl.mmad[d]);
+            return true;
+        };
+
+        if (t == 0) {
+            for (int j = 0; j < kFS && j < n; j++) issue_copy(j);
+            if (n > 0 && !issue_mma(0)) ctl.err = 1;
+        }
+        __syncthreads();
+        for (int j = 0; j < n; j++) {
+            const long long gi = gblk + j;
+            const int s = (int)(gi % kFS), d = (int)(gi & 1);
+            if (t == 0 && !ctl.err && j + 1 < n) {
+                if (!issue_mma(j + 1)) ctl.err = 2;
+            }
+            if (!mbar_wait(&ctl.mmad[d], (uint32_t)((gi >> 1) & 1), kFWait)) ctl.err = 3;
+            tc_fence_after();
+            __syncthreads();
+            if (ctl.err) break;
+            // make the record's tail visible to every thread
+            mbar_wait(&ctl.full[s], (uint32_t)((gi / kFS) & 1), kFWait);
+            const unsigned char *Bs = B0 + (size_t)s * rec_pad;
+            const int blk = split + j * splits;
+            const float *o2 = reinterpret_cast<const float *>(Bs + fs.btile_bytes);
+            const float *rn = o2 + 128;
+            const float cn = o2[256];
+            const int nvalid = reinterpret_cast<const int *>(o2)[257];
+            const uint32_t taddr = tmem + ((uint32_t)(warp & 3) * 32u << 16) + (uint32_t)(d * 256);
+            float v[16];
+            tmem_ld16(taddr + 128, v);
+            const float qc = v[0] + v[1] + v[2];
+            const float ec = 2.f * kEpsC * qn * cn + 1e-6f;
+            // lb = (|q|^2 - 2 q.c - ec - 2e-6 |q|^2) + |o|^2 (1 - 2e-6) - cq |r| - 2 q.r
+            const float t0 = q2 - 2.f * qc - ec - 2e-6f * q2;
+#pragma unroll 1
+            for (int c = g * CW; c < (g + 1) * CW; c += 16) {
+                tmem_ld16(taddr + (uint32_t)c, v);
+                if (qi < 0) continue;
+#pragma unroll
+                for (int u = 0; u < 16; u++) {
+                    const int jj = c + u;
+                    if (jj >= nvalid) break;
+                    const float oo = o2[jj], rr = rn[jj];
+                    const float lb = fmaf(-2.f, v[u], fmaf(-cq, rr, fmaf(oo, 0.999998f, t0)));
+                    if (lb <= R2) {
+                        if (MODE != 0) {
+                            int sl = atomicAdd(&a.cand_cnt[qi], 1);
+                            if (sl < kFCand) {
+                                a.cand_pos[(size_t)qi * kFCand + sl] = blk * kFB + jj;
+                                a.cand_lb[(size_t)qi * kFCand + sl] = lb;
+                            }
+                            appended++;
                         }
-                        appended++;
-                    }
-                    const float ub = lb + 2.f * fmaf(cq, rr, ec + 2e-6f * (q2 + oo));
-                    if (ub < R2) {   // replace the largest of the k kept bounds
-                        heap[hidx * NT + t] = ub;
-                        float mx = -1.f;
-                        for (int h = 0; h < k; h++) {
-                            float hv = heap[h * NT + t];
-                            if (hv > mx) { mx = hv; hidx = h; }
+                        if (MODE != 1) {
+                            const float ub = lb + 2.f * fmaf(cq, rr, ec + 2e-6f * (q2 + oo));
+                            if (ub < R2) {   // replace the largest of the k kept bounds
+                                heap[hidx * NT + t] = ub;
+                                float mx = -1.f;
+                                for (int h = 0; h < k; h++) {
+                                    float hv = heap[h * NT + t];
+                                    if (hv > mx) { mx = hv; hidx = h; }
+                                }
+                                R2 = fminf(mx, seed);
+                            }
                         }
-                        R2 = fminf(mx, seed);
                     }
                 }
             }
+            blocks_done++;
+            tc_fence_before();
+            __syncthreads();
+            if (t == 0 && j + kFS < n) issue_copy(j + kFS);
         }
-        blocks_done++;
+        gblk += n;
+        if (MODE != 1 && qi >= 0) {
+            float *dst = a.hbuf + (((size_t)qi * splits + split) * CG + g) * k;
+            for (int h = 0; h < k; h++) dst[h] = heap[h * NT + t];
+        }
         tc_fence_before();
         __syncthreads();
-        if (t == 0 && i + 2 < nseq) issue_copy(i + 2);
-    }
-    __syncthreads();
-    if (g == 0 && qi >= 0) {
-        // k-th smallest of the union of this query's CG heaps (no object is
-        // in two of them), capped by the seed
-        float vals[64];
-        int nv = 0;
-        for (int gg = 0; gg < CG; gg++)
-            for (int h = 0; h < k; h++) vals[nv++] = heap[h * NT + lq + 128 * gg];
-        float kth = FLT_MAX;
-        for (int r = 0; r < k; r++) {   // partial selection of the k smallest
-            int mi = r;
-            for (int x = r + 1; x < nv; x++)
-                if (vals[x] < vals[mi]) mi = x;
-            float tmp = vals[r];
-            vals[r] = vals[mi];
-            vals[mi] = tmp;
-        }
-        kth = vals[k - 1];
-        float bound = fminf(kth, seed);
-        atomicMin(&a.r2_bits[qi], __float_as_int(bound > 0.f ? bound : 0.f));
     }
     if (a.stats && appended) atomicAdd(&a.stats[5], appended);
-    if (t == 0) {
-        if (ctl.err) {
-            atomicMax(a.status, 16 + ctl.err);
-            // let copies still in flight land before the CTA leaves (bounded)
-            for (int s = 0; s < 2; s++)
-                for (int n = ctl.done[s]; n < ctl.pend[s]; n++) mbar_wait(&ctl.full[s], n & 1, kFWait);
-        }
-        if (a.stats) {
-            atomicAdd(&a.stats[0], blocks_done);
-            atomicAdd(&a.stats[1], (unsigned long long)fs.rec_bytes * blocks_done);
-        }
+    if (a.stats && blocks_done && t == 0) {
+        atomicAdd(&a.stats[0], blocks_done);
+        atomicAdd(&a.stats[1], (unsigned long long)fs.rec_bytes * blocks_done);
+    }
+    if (t == 0 && ctl.err) {
+        atomicMax(a.status, 16 + ctl.err);
+        // let copies still in flight land before the CTA leaves (bounded)
+        for (int s = 0; s < kFS; s++)
+            for (int m = ctl.done[s]; m < ctl.pend[s]; m++) mbar_wait(&ctl.full[s], (uint32_t)(m & 1), kFWait);
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, 512);
 }
 
+// Bound merge: the k-th smallest of every upper bound a query's threads kept
+// in the bound pass (no object appears twice: each block belongs to one
+// split and each column to one group), capped by any seed already there.
+__global__ void __launch_bounds__(128) k_fast_merge(const float *__restrict__ hbuf, int per_query, int k,
+                                                    int *__restrict__ r2_bits)
+{
+    __shared__ float v[1024];
+    const int q = blockIdx.x, t = threadIdx.x;
+    int p2 = 1;
+    while (p2 < per_query) p2 <<= 1;
+    for (int i = t; i < p2; i += 128) v[i] = i < per_query ? hbuf[(size_t)q * per_query + i] : FLT_MAX;
+    __syncthreads();
+    for (int size = 2; size <= p2; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = t; i < p2 / 2; i += 128) {
+                int lo = 2 * i - (i & (stride - 1)), hi = lo + stride;
+                bool up = (lo & size) == 0;
+                float a = v[lo], b = v[hi];
+                if ((a > b) == up) {
+                    v[lo] = b;
+                    v[hi] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (t == 0) {
+        float kth = v[k - 1];
+        atomicMin(&r2_bits[q], __float_as_int(kth > 0.f ? kth : 0.f));
+    }
+}
+
 // ---------------------------------------------------------------- finalize
 
-constexpr int kFinSort = 1024;
+constexpr int kFinSort = kFCand;
 
 // One CTA per query: exact values of the surviving candidates, de-duplicated,
 // top k by (distance, id).  Sets overflow[q] when the list was truncated.
@@ -564,23 +569,30 @@ __global__ void k_scatter_results(const int *idx, int n, int k, const float *kth
 
 // Column groups per query lane: as many warps as the bound heaps
 // (threads x k floats, at most 32 KB of shared memory) allow.
-template <int CG>
-static int launch_fast_tile_cg(const FastTileArgs &a, int ntiles, int splits, cudaStream_t st)
+static int fast_cg(int k) { return k <= 16 ? 4 : (k <= 32 ? 2 : 1); }
+
+template <int CG, int MODE>
+static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
 {
     const uint32_t rec_pad = (a.fs.rec_bytes + 1023u) & ~1023u;
-    size_t smem = 1024 + 2 * (size_t)a.fs.atile_bytes + 2 * (size_t)rec_pad +
-                  sizeof(float) * 128 * CG * (size_t)a.k + sizeof(FastCtl) + 64;
-    GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_tile<CG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_fast_tile<CG><<<dim3(ntiles, splits), 128 * CG, smem, st>>>(a);
+    size_t smem = 1024 + 2 * (size_t)a.fs.atile_bytes + kFS * (size_t)rec_pad +
+                  (MODE == 1 ? 0 : sizeof(float) * 128 * CG * (size_t)a.k) + sizeof(FastCtl) + 64;
+    GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_tile<CG, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    GTS_CUDA_TRY(cudaMemsetAsync(a.item_counter, 0, sizeof(int), st));
+    k_fast_tile<CG, MODE><<<grid, 128 * CG, smem, st>>>(a);
     GTS_CUDA_TRY(cudaGetLastError());
     return GTS_OK;
 }
 
-static int launch_fast_tile(const FastTileArgs &a, int ntiles, int splits, cudaStream_t st)
+template <int MODE>
+static int launch_fast_tile(const FastTileArgs &a, int grid, cudaStream_t st)
 {
-    if (a.k <= 16) return launch_fast_tile_cg<4>(a, ntiles, splits, st);
-    if (a.k <= 32) return launch_fast_tile_cg<2>(a, ntiles, splits, st);
-    return launch_fast_tile_cg<1>(a, ntiles, splits, st);
+    switch (fast_cg(a.k)) {
+    case 4: return launch_fast_tile_cg<4, MODE>(a, grid, st);
+    case 2: return launch_fast_tile_cg<2, MODE>(a, grid, st);
+    default: return launch_fast_tile_cg<1, MODE>(a, grid, st);
+    }
 }
 
 bool fast_supported(const gts_index *idx, int k)
@@ -606,22 +618,28 @@ static int fast_prepare(gts_index *idx, cudaStream_t st)
     return GTS_OK;
 }
 
-int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
-                    float *d_dists, cudaStream_t st)
+// One filter run over a query batch.  seeded: take each query's starting
+// bound from the learned radius model and make a single appending pass;
+// otherwise a bound-only pass first.  Queries the run cannot answer (a
+// seed below the k-th distance, or a full candidate list) are written to
+// d_fail (owned by the caller) and counted in *n_fail.
+static int fast_run(gts_index *idx, const int *d_qids, int qnum, int k, bool seeded, float *d_kth, int *d_ids,
+                    float *d_dists, int *d_fail, int *n_fail, cudaStream_t st)
 {
-    int rc = fast_prepare(idx, st);
-    if (rc) return rc;
     const FastShape fs = fast_shape(idx->dim);
     const int ntiles = (qnum + kFT - 1) / kFT;
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    int splits = (nsm + ntiles - 1) / ntiles;
+    // items = tiles x splits, about four per SM for balance; the bound merge
+    // holds splits * CG * k <= 1024 values per query
+    const int cg = fast_cg(k);
+    int splits = (4 * nsm + ntiles - 1) / ntiles;
     if (splits < 1) splits = 1;
-    if (splits > 8) splits = 8;
+    if (splits > 1024 / (cg * k)) splits = 1024 / (cg * k);
     if (splits > idx->fast_nb) splits = idx->fast_nb;
+    const int grid = std::min(nsm, ntiles * splits);
 
-    // scratch: keys, vals, sorted keys, order, cand_pos, cand_lb, cand_cnt, r2, overflow, n_overflow, cub temp
     size_t cub_bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (int *)nullptr, (int *)nullptr, (int *)nullptr,
                                     (int *)nullptr, qnum, 0, 32, st);
@@ -631,22 +649,23 @@ int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d
     size_t o_skeys = take(sizeof(int) * qnum), o_order = take(sizeof(int) * qnum);
     size_t o_cpos = take(sizeof(int) * (size_t)qnum * kFCand), o_clb = take(sizeof(float) * (size_t)qnum * kFCand);
     size_t o_ccnt = take(sizeof(int) * qnum), o_r2 = take(sizeof(int) * qnum);
-    size_t o_ovf = take(sizeof(int) * qnum), o_novf = take(sizeof(int));
+    size_t o_novf = take(sizeof(int)), o_items = take(sizeof(int));
+    size_t o_hbuf = take(sizeof(float) * (size_t)qnum * splits * cg * k);
     size_t o_cub = take(cub_bytes);
+    int rc;
     if ((rc = ensure_scratch(idx, off))) return rc;
     unsigned char *S = (unsigned char *)idx->scratch;
     int *keys = (int *)(S + o_keys), *vals = (int *)(S + o_vals), *skeys = (int *)(S + o_skeys);
     int *order = (int *)(S + o_order), *cpos = (int *)(S + o_cpos), *ccnt = (int *)(S + o_ccnt);
     float *clb = (float *)(S + o_clb);
-    int *r2 = (int *)(S + o_r2), *ovf = (int *)(S + o_ovf), *novf = (int *)(S + o_novf);
+    int *r2 = (int *)(S + o_r2), *novf = (int *)(S + o_novf);
 
     k_fast_keys<<<(qnum + 255) / 256, 256, 0, st>>>(d_qids, qnum, idx->pos_of_id, keys, vals);
     size_t cb = cub_bytes;
     GTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(S + o_cub, cb, keys, skeys, vals, order, qnum, 0, 32, st));
     k_fast_init<<<(qnum + 255) / 256, 256, 0, st>>>(qnum, ccnt, r2);
+    if (seeded && (rc = mlp_seed(idx, d_qids, qnum, k, r2, st))) return rc;
     GTS_CUDA_TRY(cudaMemsetAsync(novf, 0, sizeof(int), st));
-    GTS_CUDA_TRY(cudaMemsetAsync(idx->d_status, 0, sizeof(int), st));
-    GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, kStatsN * sizeof(unsigned long long), st));
 
     FastTileArgs a;
     a.rows = idx->rows;
@@ -664,47 +683,84 @@ int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d
     a.cand_lb = clb;
     a.cand_cnt = ccnt;
     a.r2_bits = r2;
+    a.hbuf = (float *)(S + o_hbuf);
+    a.item_counter = (int *)(S + o_items);
+    a.ntiles = ntiles;
     a.status = idx->d_status;
     a.stats = idx->d_stats;
-    // pass 1 only tightens every query's k-th bound; pass 2 appends the
-    // objects whose lower bound falls within it (without pass 1 the early
-    // blocks would append everything below a still-loose radius)
-    a.append = 0;
-    if ((rc = launch_fast_tile(a, ntiles, splits, st))) return rc;
-    a.append = 1;
-    if ((rc = launch_fast_tile(a, ntiles, splits, st))) return rc;
-    k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 2ull);
+    // seeded: one pass that appends within min(seed, running k-th bound) and
+    // keeps the bounds; otherwise a bound pass first, then an appending one.
+    // The merge lowers each query's bound to the k-th smallest kept bound.
+    if ((rc = seeded ? launch_fast_tile<2>(a, grid, st) : launch_fast_tile<0>(a, grid, st))) return rc;
+    k_fast_merge<<<qnum, 128, 0, st>>>(a.hbuf, splits * cg * k, k, r2);
+    GTS_CUDA_TRY(cudaGetLastError());
+    if (!seeded && (rc = launch_fast_tile<1>(a, grid, st))) return rc;
+    k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, seeded ? 1ull : 2ull);
     k_fast_final<<<qnum, 128, 0, st>>>(idx->rows, idx->dim, idx->num, idx->id_list, d_qids, qnum, k,
                                         idx->params.infi_dis, cpos, clb, ccnt, r2, d_kth, d_ids, d_dists,
-                                        ovf, novf, idx->d_stats);
+                                        d_fail, novf, idx->d_stats);
     GTS_CUDA_TRY(cudaGetLastError());
-    int status = 0, n_ovf = 0;
+    int status = 0;
     GTS_CUDA_TRY(cudaMemcpyAsync(&status, idx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
-    GTS_CUDA_TRY(cudaMemcpyAsync(&n_ovf, novf, sizeof(int), cudaMemcpyDeviceToHost, st));
+    GTS_CUDA_TRY(cudaMemcpyAsync(n_fail, novf, sizeof(int), cudaMemcpyDeviceToHost, st));
     GTS_CUDA_TRY(cudaStreamSynchronize(st));
     if (status != 0) {
         gts_set_error("tensor-core filter kernel reported status %d (barrier wait gave up)", status);
         return GTS_ERR_KERNEL;
     }
-    if (n_ovf > 0) {   // candidate lists that overflowed: answer those queries on the plain path
-        int *sub_q = nullptr, *sub_ids = nullptr;
-        float *sub_kth = nullptr, *sub_dis = nullptr;
-        DevVec keep;
-        if ((rc = keep.alloc(&sub_q, n_ovf)) || (rc = keep.alloc(&sub_kth, n_ovf)) ||
-            (d_ids && (rc = keep.alloc(&sub_ids, (size_t)n_ovf * k))) ||
-            (d_dists && (rc = keep.alloc(&sub_dis, (size_t)n_ovf * k))))
+    return GTS_OK;
+}
+
+// Queries listed in d_fail (indices into d_qids) answered again: unseeded
+// filter first when the first run was seeded, the plain traversal last.
+static int rerun_failed(gts_index *idx, const int *d_qids, int k, bool was_seeded, const int *d_fail, int n_fail,
+                        float *d_kth, int *d_ids, float *d_dists, cudaStream_t st)
+{
+    int *sub_q = nullptr, *sub_ids = nullptr, *sub_fail = nullptr, *fail_copy = nullptr;
+    float *sub_kth = nullptr, *sub_dis = nullptr;
+    DevVec keep;
+    int rc;
+    if ((rc = keep.alloc(&sub_q, n_fail)) || (rc = keep.alloc(&sub_kth, n_fail)) ||
+        (rc = keep.alloc(&fail_copy, n_fail)) || (rc = keep.alloc(&sub_fail, n_fail)) ||
+        (d_ids && (rc = keep.alloc(&sub_ids, (size_t)n_fail * k))) ||
+        (d_dists && (rc = keep.alloc(&sub_dis, (size_t)n_fail * k))))
+        return rc;
+    GTS_CUDA_TRY(cudaMemcpyAsync(fail_copy, d_fail, sizeof(int) * n_fail, cudaMemcpyDeviceToDevice, st));
+    k_gather_i<<<(n_fail + 255) / 256, 256, 0, st>>>(d_qids, fail_copy, n_fail, sub_q);
+    if (was_seeded) {
+        int n2 = 0;
+        if ((rc = fast_run(idx, sub_q, n_fail, k, false, sub_kth, sub_ids, sub_dis, sub_fail, &n2, st))) return rc;
+        if (n2 > 0 && (rc = rerun_failed(idx, sub_q, k, false, sub_fail, n2, sub_kth, sub_ids, sub_dis, st)))
             return rc;
-        k_gather_i<<<(n_ovf + 255) / 256, 256, 0, st>>>(d_qids, ovf, n_ovf, sub_q);
-        k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 4, (unsigned long long)n_ovf);
+    } else {
+        k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 4, (unsigned long long)n_fail);
         idx->keep_stats = true;
-        rc = search_knn(idx, sub_q, n_ovf, k, 0, sub_kth, sub_ids, sub_dis, st);
+        rc = search_knn(idx, sub_q, n_fail, k, 0, sub_kth, sub_ids, sub_dis, st);
         idx->keep_stats = false;
         if (rc) return rc;
-        k_scatter_results<<<(n_ovf + 255) / 256, 256, 0, st>>>(ovf, n_ovf, k, sub_kth, sub_ids, sub_dis, d_kth,
-                                                              d_ids, d_dists);
-        GTS_CUDA_TRY(cudaStreamSynchronize(st));
     }
-    idx->last_fast_overflow = n_ovf;
+    k_scatter_results<<<(n_fail + 255) / 256, 256, 0, st>>>(fail_copy, n_fail, k, sub_kth, sub_ids, sub_dis, d_kth,
+                                                           d_ids, d_dists);
+    GTS_CUDA_TRY(cudaGetLastError());
+    GTS_CUDA_TRY(cudaStreamSynchronize(st));
+    return GTS_OK;
+}
+
+int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
+                    float *d_dists, cudaStream_t st)
+{
+    int rc = fast_prepare(idx, st);
+    if (rc) return rc;
+    GTS_CUDA_TRY(cudaMemsetAsync(idx->d_status, 0, sizeof(int), st));
+    GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, kStatsN * sizeof(unsigned long long), st));
+    const bool seeded = idx->mlp_ready;
+    DevVec keep;
+    int *fail = nullptr;
+    if ((rc = keep.alloc(&fail, qnum))) return rc;
+    int n_fail = 0;
+    if ((rc = fast_run(idx, d_qids, qnum, k, seeded, d_kth, d_ids, d_dists, fail, &n_fail, st))) return rc;
+    idx->last_fast_overflow = n_fail;
+    if (n_fail > 0) return rerun_failed(idx, d_qids, k, seeded, fail, n_fail, d_kth, d_ids, d_dists, st);
     return GTS_OK;
 }
 

@@ -35,6 +35,14 @@ struct gts_index {
     void *scratch = nullptr;
     size_t scratch_bytes = 0;
 
+    // learned kNN radius (mlp.cu): parameters, input standardisation,
+    // feature pivots; valid for the tree it was trained on
+    float *mlp_P = nullptr, *mlp_norm = nullptr;
+    int *mlp_piv = nullptr;
+    int mlp_npiv = 0;
+    float mlp_ymu = 0.f, mlp_ysig = 1.f, mlp_widen = 1.f;
+    bool mlp_ready = false;
+
     gts::DevTree dev() const;
 };
 
@@ -68,6 +76,7 @@ int dev_alloc(T **p, size_t n, size_t *acct);
 int ensure_scratch(gts_index *idx, size_t bytes);
 
 bool fast_supported(const gts_index *idx, int k);
+int mlp_seed(gts_index *idx, const int *d_qids, int qnum, int k, int *d_r2_bits, cudaStream_t st);
 int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                     float *d_dists, cudaStream_t s);
 

@@ -164,6 +164,50 @@ __device__ __forceinline__ float warp_row_value(const float *__restrict__ row,
     return metric == kLinf ? warp_max(acc) : warp_sum(acc);
 }
 
+// Four rows at once (independent loads in flight): out[u] as warp_row_value.
+__device__ __forceinline__ void warp_row_value4(const float *const (&rows)[4], const float *__restrict__ q,
+                                                int dim, int metric, int lane, float (&out)[4])
+{
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    if ((dim & 3) == 0) {
+        const float4 *q4 = reinterpret_cast<const float4 *>(q);
+        for (int j = lane; j < (dim >> 2); j += 32) {
+            float4 x[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) x[u] = __ldg(reinterpret_cast<const float4 *>(rows[u]) + j);
+            const float4 y = q4[j];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                float d0 = x[u].x - y.x, d1 = x[u].y - y.y, d2 = x[u].z - y.z, d3 = x[u].w - y.w;
+                if (metric == kL2) {
+                    acc[u] = fmaf(d0, d0, acc[u]); acc[u] = fmaf(d1, d1, acc[u]);
+                    acc[u] = fmaf(d2, d2, acc[u]); acc[u] = fmaf(d3, d3, acc[u]);
+                } else if (metric == kL1) {
+                    acc[u] += fabsf(d0) + fabsf(d1) + fabsf(d2) + fabsf(d3);
+                } else {
+                    acc[u] = fmaxf(acc[u], fmaxf(fmaxf(fabsf(d0), fabsf(d1)), fmaxf(fabsf(d2), fabsf(d3))));
+                }
+            }
+        }
+    } else {
+        for (int j = lane; j < dim; j += 32) {
+            float x[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) x[u] = __ldg(rows[u] + j);
+            const float y = q[j];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                float d0 = x[u] - y;
+                if (metric == kL2) acc[u] = fmaf(d0, d0, acc[u]);
+                else if (metric == kL1) acc[u] += fabsf(d0);
+                else acc[u] = fmaxf(acc[u], fabsf(d0));
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) out[u] = metric == kLinf ? warp_max(acc[u]) : warp_sum(acc[u]);
+}
+
 // Interval [lo, hi] that contains both exact leaf values (F32 and F64
 // sites) given the FP32 warp value v.
 __device__ __forceinline__ void value_bounds(int metric, int dim, float v, double &lo, double &hi)
@@ -323,30 +367,38 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
             // ---- leaves: filter every object, collect those needing exact values
             if (nleaf > 0) {
                 if (warp_filter) {
-                    for (int o = warp; o < nobj; o += kWarps) {
-                        int li = 0;
-                        while (s.leaf_pre[li + 1] <= o) li++;
-                        int pos = t.node_lid[s.bleaf[li]] + s.bleaf_off[li] + (o - s.leaf_pre[li]);
-                        int id = t.id_list[pos];
-                        if (is_deleted(a.deleted, id)) continue;
-                        float v = warp_row_value(t.trows + (size_t)pos * t.dim, qrow, t.dim, t.metric, lane);
+                    // four rows per warp step: their loads are in flight together
+                    for (int o0 = warp * 4; o0 < nobj; o0 += kWarps * 4) {
+                        int pos[4], id[4];
+                        const float *rp[4];
+#pragma unroll
+                        for (int u = 0; u < 4; u++) {
+                            int o = min(o0 + u, nobj - 1);
+                            int li = 0;
+                            while (s.leaf_pre[li + 1] <= o) li++;
+                            pos[u] = t.node_lid[s.bleaf[li]] + s.bleaf_off[li] + (o - s.leaf_pre[li]);
+                            id[u] = t.id_list[pos[u]];
+                            rp[u] = t.trows + (size_t)pos[u] * t.dim;
+                        }
+                        float v4[4];
+                        warp_row_value4(rp, qrow, t.dim, t.metric, lane, v4);
                         if (lane == 0) {
-                            if (id == qid) {
-                                v = 0.f;
-                            }
-                            double lo, hi;
-                            value_bounds(t.metric, t.dim, v, lo, hi);
-                            if (id == qid) lo = hi = 0.0;
-                            if (knn) {
-                                if (lo <= s.R) {
+                            for (int u = 0; u < 4 && o0 + u < nobj; u++) {
+                                if (is_deleted(a.deleted, id[u])) continue;
+                                double lo, hi;
+                                value_bounds(t.metric, t.dim, v4[u], lo, hi);
+                                if (id[u] == qid) lo = hi = 0.0;
+                                if (knn) {
+                                    if (lo <= s.R) {
+                                        int c = atomicAdd(&s.ncpos, 1);
+                                        s.cpos[c] = pos[u];
+                                    }
+                                } else if (a.mode == kModeRangeCount && hi < (double)a.r * (1.0 - 2.4e-7)) {
+                                    atomicAdd(&s.cnt, 1);
+                                } else if (lo <= (double)a.r * (1.0 + 2.4e-7)) {
                                     int c = atomicAdd(&s.ncpos, 1);
-                                    s.cpos[c] = pos;
+                                    s.cpos[c] = pos[u];
                                 }
-                            } else if (a.mode == kModeRangeCount && hi < (double)a.r * (1.0 - 2.4e-7)) {
-                                atomicAdd(&s.cnt, 1);
-                            } else if (lo <= (double)a.r * (1.0 + 2.4e-7)) {
-                                int c = atomicAdd(&s.ncpos, 1);
-                                s.cpos[c] = pos;
                             }
                         }
                     }

@@ -150,6 +150,34 @@ int gts_range_device(gts_index *idx, const int *d_qids, int qnum, float r,
 int gts_range_ids(gts_index *idx, const int *qids, int qnum, float r, int *counts_out,
                   int *offsets_out, int *ids_out, float *dists_out, size_t capacity);
 
+/* ---------------------------------------------------------------- learned radius */
+
+/* No reference counterpart (the reference has no learned component).
+ * Train the kNN radius predictor of an L2 index: a 33-128-128-1 MLP whose
+ * inputs are a query's distances to the first 32 pivots of the tree plus
+ * log(k), and whose output is log of the k-th neighbour distance.  Labels are
+ * exact radii of n_train random objects (k drawn from {1, 8, 32, 64} up to
+ * k_max) computed by this index's own exact search; training runs on the
+ * device (forward, backward and Adam kernels).  Afterwards GTS_FORM_FAST
+ * searches start from the predicted radius, widened by the 99th percentile
+ * of the held-out under-predictions, and re-answer any query whose radius
+ * held fewer than k objects -- results stay exact.
+ * val_rmse_log: RMS error of log(radius) on the held-out 10%; widen: factor
+ * applied to predictions (both nullable).  A rebuild discards the model. */
+int gts_learn_radius(gts_index *idx, int n_train, int k_max, int epochs, unsigned seed,
+                     float *val_rmse_log, float *widen);
+
+/* The trained model: params[20993] (W1[128][33] b1[128] W2[128][128] b2[128]
+ * W3[128] b3), norm[66] (input means, input deviations), ymu_ysig_widen[3].
+ * Each pointer may be NULL. */
+int gts_radius_model_params(const gts_index *idx, float *params, float *norm, float *ymu_ysig_widen);
+
+/* Loss and parameter gradient of the model's mean squared error on a host
+ * batch (X[batch][33] raw features, target[batch] standardised log radii),
+ * evaluated by the device training kernels. */
+int gts_radius_model_grad(const float *X, const float *target, int batch, const float *params,
+                          const float *norm, float *grad, float *loss);
+
 /* ---------------------------------------------------------------- update */
 
 /* updateIndexRnn (update.cuh:449-638): replay a stream of operations

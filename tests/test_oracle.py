@@ -151,3 +151,20 @@ def test_oracle_on_reference_sample(oracle):
     ref = np.array([int(v) for v in vals])
     got = oracle.range_v2(ds, p, t, qids, 30.0)
     assert (got != ref).sum() <= 2   # only objects within an ulp of 30 degrees may differ
+
+
+def test_radius_network_oracle_gradient_finite_differences():
+    from oracle import mlp_oracle as M
+    rng = np.random.default_rng(3)
+    P = rng.standard_normal(M.N_PARAMS) * 0.1
+    X = rng.random((40, M.N_IN))
+    norm = np.concatenate([X.mean(0), X.std(0) + 0.1])
+    t = rng.standard_normal(40)
+    _, g = M.loss_and_grad(X, t, P, norm)
+    eps = 1e-6
+    for i in [0, 777, 4300, 5000, 20900, M.N_PARAMS - 1]:
+        Pp, Pm = P.copy(), P.copy()
+        Pp[i] += eps
+        Pm[i] -= eps
+        fd = (M.loss_and_grad(X, t, Pp, norm)[0] - M.loss_and_grad(X, t, Pm, norm)[0]) / (2 * eps)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(g[i])
