@@ -623,8 +623,11 @@ static int fast_prepare(gts_index *idx, cudaStream_t st)
 // otherwise a bound-only pass first.  Queries the run cannot answer (a
 // seed below the k-th distance, or a full candidate list) are written to
 // d_fail (owned by the caller) and counted in *n_fail.
+// fixed (optional): caller-owned device scratch of fixed_bytes used instead
+// of the index's growable scratch.
 static int fast_run(gts_index *idx, const int *d_qids, int qnum, int k, bool seeded, float *d_kth, int *d_ids,
-                    float *d_dists, int *d_fail, int *n_fail, cudaStream_t st)
+                    float *d_dists, int *d_fail, int *n_fail, cudaStream_t st, unsigned char *fixed = nullptr,
+                    size_t fixed_bytes = 0)
 {
     const FastShape fs = fast_shape(idx->dim);
     const int ntiles = (qnum + kFT - 1) / kFT;
@@ -653,8 +656,16 @@ static int fast_run(gts_index *idx, const int *d_qids, int qnum, int k, bool see
     size_t o_hbuf = take(sizeof(float) * (size_t)qnum * splits * cg * k);
     size_t o_cub = take(cub_bytes);
     int rc;
-    if ((rc = ensure_scratch(idx, off))) return rc;
-    unsigned char *S = (unsigned char *)idx->scratch;
+    unsigned char *S = fixed;
+    if (fixed) {
+        if (off > fixed_bytes) {
+            gts_set_error("filter run needs %zu bytes of scratch, the fixed array holds %zu", off, fixed_bytes);
+            return GTS_ERR_INVALID;
+        }
+    } else {
+        if ((rc = ensure_scratch(idx, off))) return rc;
+        S = (unsigned char *)idx->scratch;
+    }
     int *keys = (int *)(S + o_keys), *vals = (int *)(S + o_vals), *skeys = (int *)(S + o_skeys);
     int *order = (int *)(S + o_order), *cpos = (int *)(S + o_cpos), *ccnt = (int *)(S + o_ccnt);
     float *clb = (float *)(S + o_clb);
@@ -761,6 +772,56 @@ int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d
     if ((rc = fast_run(idx, d_qids, qnum, k, seeded, d_kth, d_ids, d_dists, fail, &n_fail, st))) return rc;
     idx->last_fast_overflow = n_fail;
     if (n_fail > 0) return rerun_failed(idx, d_qids, k, seeded, fail, n_fail, d_kth, d_ids, d_dists, st);
+    return GTS_OK;
+}
+
+// The unseeded filter run with every buffer carved out of `scratch`
+// (bytes long, 256-byte aligned): no device allocation on any path.  The
+// filter records must already exist.  Queries the run could not answer
+// (a full candidate list) go to the plain traversal, which uses only the
+// index's own counters.
+int search_knn_fast_fixed(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
+                          float *d_dists, unsigned char *scratch, size_t bytes, cudaStream_t st)
+{
+    if (!fast_supported(idx, k)) {
+        gts_set_error("fixed-scratch kNN supports the L2 metric with dim <= %d and 1 <= k <= %d", kFMaxKp, kFMaxK);
+        return GTS_ERR_INVALID;
+    }
+    if (!idx->fast_recs) {
+        gts_set_error("the index has no filter records yet: one GTS_FORM_FAST kNN call on it must come first");
+        return GTS_ERR_INVALID;
+    }
+    if (qnum <= 0) return GTS_OK;
+    size_t off = 0;
+    auto take = [&](size_t b) { size_t o = off; off += (b + 255) & ~(size_t)255; return o; };
+    const size_t o_fail = take(sizeof(int) * qnum), o_subq = take(sizeof(int) * qnum);
+    const size_t o_kth = take(sizeof(float) * qnum);
+    const size_t o_ids = take(sizeof(int) * (size_t)qnum * k), o_dis = take(sizeof(float) * (size_t)qnum * k);
+    if (off > bytes) {
+        gts_set_error("fixed scratch of %zu bytes is too small for %d queries", bytes, qnum);
+        return GTS_ERR_INVALID;
+    }
+    int *fail = (int *)(scratch + o_fail), *sub_q = (int *)(scratch + o_subq);
+    float *sub_kth = (float *)(scratch + o_kth), *sub_dis = (float *)(scratch + o_dis);
+    int *sub_ids = (int *)(scratch + o_ids);
+    GTS_CUDA_TRY(cudaMemsetAsync(idx->d_status, 0, sizeof(int), st));
+    GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, kStatsN * sizeof(unsigned long long), st));
+    int n_fail = 0, rc;
+    if ((rc = fast_run(idx, d_qids, qnum, k, false, d_kth, d_ids, d_dists, fail, &n_fail, st, scratch + off,
+                       bytes - off)))
+        return rc;
+    idx->last_fast_overflow = n_fail;
+    if (n_fail == 0) return GTS_OK;
+    k_gather_i<<<(n_fail + 255) / 256, 256, 0, st>>>(d_qids, fail, n_fail, sub_q);
+    k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 4, (unsigned long long)n_fail);
+    idx->keep_stats = true;
+    rc = search_knn(idx, sub_q, n_fail, k, 0, sub_kth, d_ids ? sub_ids : nullptr, d_dists ? sub_dis : nullptr, st);
+    idx->keep_stats = false;
+    if (rc) return rc;
+    k_scatter_results<<<(n_fail + 255) / 256, 256, 0, st>>>(fail, n_fail, k, sub_kth, d_ids ? sub_ids : nullptr,
+                                                           d_dists ? sub_dis : nullptr, d_kth, d_ids, d_dists);
+    GTS_CUDA_TRY(cudaGetLastError());
+    GTS_CUDA_TRY(cudaStreamSynchronize(st));
     return GTS_OK;
 }
 

@@ -79,6 +79,9 @@ bool fast_supported(const gts_index *idx, int k);
 int mlp_seed(gts_index *idx, const int *d_qids, int qnum, int k, int *d_r2_bits, cudaStream_t st);
 int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                     float *d_dists, cudaStream_t s);
+// Unseeded filter with all scratch inside the caller's fixed buffer.
+int search_knn_fast_fixed(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
+                          float *d_dists, unsigned char *scratch, size_t bytes, cudaStream_t s);
 
 // A set of device allocations freed together on scope exit.
 struct DevVec {

@@ -135,6 +135,18 @@ int gts_knn(gts_index *idx, const int *qids, int qnum, int k, int form,
 int gts_knn_device(gts_index *idx, const int *d_qids, int qnum, int k, int form,
                    float *d_kth, int *d_ids, float *d_dists, void *stream);
 
+/* No counterpart in the reference.  gts_knn_device's GTS_FORM_FAST results
+ * (the unseeded BF16 filter + exact recheck) without any device allocation:
+ * scratch is a fixed 12 MiB file-scope device array per device, so at most
+ * 512 queries per call (more -> GTS_ERR_INVALID), L2 only, dim <= 128,
+ * 1 <= k <= 64.  The index must already hold its filter records (made by
+ * one earlier GTS_FORM_FAST gts_knn / gts_knn_device call).  The first call
+ * on a device looks the array up (cudaGetSymbolAddress) and should come
+ * before any stream capture.  All calls on a device share the array: calls
+ * that overlap on the GPU race. */
+int gts_knn_device_noalloc(gts_index *idx, const int *d_qids, int qnum, int k,
+                           float *d_kth, int *d_ids, float *d_dists, void *stream);
+
 /* searchIndexRnnV2 (search_v2.cuh:780-972) -> res.
  * counts_out[q]: number of objects within r of qids[q] (itself included). */
 int gts_range(gts_index *idx, const int *qids, int qnum, float r, int *counts_out);
