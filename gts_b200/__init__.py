@@ -258,8 +258,18 @@ class Index:
         _check(self._lib.gts_search_stats(self._h, out))
         return {"objects": out[0], "pivots": out[1], "exact": out[2], "queries": out[3],
                 "fallback": out[4], "appended": out[5], "passes": out[6],
-                # fast form: [0] counts operand blocks and [1] their bytes
-                "blocks": out[0], "bytes": out[1]}
+                # fast form: [0] counts operand blocks and [1] their bytes;
+                # [7] the (query tile, block) pairs the block bound tested
+                "blocks": out[0], "bytes": out[1], "tested": out[7]}
+
+    def filter_timing(self, reset: bool = False):
+        """(milliseconds, launches) of the fast form's filter kernel since the
+        last reset, from CUDA events around each launch; reset=True zeroes
+        the totals and turns the timing on."""
+        ms = C.c_double()
+        n = C.c_longlong()
+        _check(self._lib.gts_filter_timing(self._h, 1 if reset else 0, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
 
     def knn(self, qids, k: int, form: int = FORM_PLAIN, return_ids: bool = False):
         q = np.ascontiguousarray(qids, dtype=np.int32)

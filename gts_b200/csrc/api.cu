@@ -382,6 +382,8 @@ extern "C" void gts_index_free(gts_index *idx)
     if (idx->mlp_P) cudaFree(idx->mlp_P);
     if (idx->mlp_norm) cudaFree(idx->mlp_norm);
     if (idx->mlp_piv) cudaFree(idx->mlp_piv);
+    for (int i = 0; i < 2; i++)
+        if (idx->fev[i]) cudaEventDestroy(idx->fev[i]);
     delete idx;
 }
 
@@ -392,6 +394,24 @@ extern "C" int gts_search_stats(const gts_index *idx, unsigned long long *out8)
         return GTS_ERR_INVALID;
     }
     GTS_CUDA_TRY(cudaMemcpy(out8, idx->d_stats, gts::kStatsN * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    return GTS_OK;
+}
+
+extern "C" int gts_filter_timing(gts_index *idx, int reset, double *ms, long long *launches)
+{
+    if (!idx) {
+        gts_set_error("null argument");
+        return GTS_ERR_INVALID;
+    }
+    if (reset) {
+        for (int i = 0; i < 2; i++)
+            if (!idx->fev[i]) GTS_CUDA_TRY(cudaEventCreate(&idx->fev[i]));
+        idx->filter_ms = 0.0;
+        idx->filter_launches = 0;
+        idx->time_filter = true;
+    }
+    if (ms) *ms = idx->filter_ms;
+    if (launches) *launches = idx->filter_launches;
     return GTS_OK;
 }
 

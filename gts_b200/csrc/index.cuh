@@ -30,6 +30,12 @@ struct gts_index {
     unsigned char *fast_recs = nullptr;
     int fast_nb = 0;
     int last_fast_overflow = 0;
+    // device time of the filter kernel (CUDA events around each launch),
+    // kept only while timing is on (gts_filter_timing)
+    bool time_filter = false;
+    cudaEvent_t fev[2] = {nullptr, nullptr};
+    double filter_ms = 0.0;
+    long long filter_launches = 0;
 
     // reusable per-call scratch (grown on demand, freed with the handle)
     void *scratch = nullptr;
@@ -54,6 +60,7 @@ namespace gts {
 //   [2] exact (reference-order) values    [3] plain: queries finished
 //   [4] fast: queries answered again on the plain path
 //   [5] fast: candidates appended         [6] fast: filter passes
+//   [7] fast: (query tile, block) pairs tested by the block bound
 constexpr int kStatsN = 8;
 
 // Build the tree for the data already placed in idx->rows / strs / lens.

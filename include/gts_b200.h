@@ -118,8 +118,15 @@ int gts_index_set_stream(gts_index *idx, void *stream);
  * out8[3] queries finished by the plain traversal
  * out8[4] fast form: queries answered again on the plain path
  * out8[5] fast form: candidates appended
- * out8[6] fast form: filter passes over the blocks; out8[7] reserved */
+ * out8[6] fast form: filter passes over the blocks
+ * out8[7] fast form: (query tile, block) pairs tested by the block bound */
 int gts_search_stats(const gts_index *idx, unsigned long long *out8);
+
+/* No counterpart in the reference.  Device time of the fast form's filter
+ * kernel, from CUDA events around each launch on the index's stream.
+ * reset != 0 zeroes the totals and turns timing on (creating the events);
+ * *ms / *launches (nullable) receive the totals since the last reset. */
+int gts_filter_timing(gts_index *idx, int reset, double *ms, long long *launches);
 
 /* ---------------------------------------------------------------- search */
 
