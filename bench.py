@@ -254,6 +254,8 @@ def run_gts(args):
           for _ in range(args.steps)]
     if args.form == "fast":
         idx.filter_timing(reset=True)
+    if args.profile:
+        torch.cuda.profiler.start()
     with ClockSampler(local) as clocks:
         t_start = torch.cuda.Event(enable_timing=True)
         t_end = torch.cuda.Event(enable_timing=True)
@@ -264,6 +266,8 @@ def run_gts(args):
             ev[i][1].record(stream)
         t_end.record(stream)
         torch.cuda.synchronize()
+    if args.profile:
+        torch.cuda.profiler.stop()
     total_ms = t_start.elapsed_time(t_end)
     per_launch_ms = [a.elapsed_time(b) for a, b in ev]
     filter_ms, filter_launches = idx.filter_timing() if args.form == "fast" else (0.0, 0)
@@ -376,6 +380,8 @@ def main():
     ap.add_argument("--no-learn", action="store_true",
                     help="fast form without the learned radius (own-block seeds only)")
     ap.add_argument("--train", type=int, default=200_000, help="learned-radius training samples")
+    ap.add_argument("--profile", action="store_true",
+                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
