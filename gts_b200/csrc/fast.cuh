@@ -1,0 +1,121 @@
+// fast.cuh -- layout shared by the tensor-core kNN filter (fast.cu) and the
+// construction of its block order (fast_order.cu).
+//
+// The filter groups objects into blocks of at most 128 (padded to 128
+// slots), and blocks into superblocks.  A slot is block * 128 + lane; slot_of
+// maps an object id to its slot, id_of_slot the reverse (-1 for padding).
+#pragma once
+#include <stdint.h>
+#include "index.cuh"
+
+namespace gts {
+
+constexpr int kFB = 128;              // slots per block
+constexpr int kFN = 144;              // B rows per block: objects + centre rows + padding
+constexpr int kFT = 128;              // queries per tile (A rows, TMEM lanes)
+constexpr int kFMaxKp = 128;          // padded dimension limit of this path (shared-memory budget)
+constexpr int kFMaxK = 64;
+
+// Block order (hierarchical k-means, fast_order.cu):
+constexpr int kOrdBranch = 16;        // k-means children per split at most
+constexpr int kOrdHalve = 1024;       // segments up to this size are halved instead
+constexpr int kOrdIters = 6;          // Lloyd iterations per level
+constexpr int kOrdSbMax = 4096;       // a superblock: the first segment of at most this many objects
+constexpr int kOrdMaxLevels = 64;
+
+struct FastShape {
+    int kp, nk;              // padded dim, number of 64-wide K chunks
+    uint32_t btile_bytes;    // nk * kFN * 128
+    uint32_t rec_bytes;      // btile_bytes + 1024 (w, dn) + 32 (block scalars)
+    uint32_t atile_bytes;    // nk * kFT * 128
+    uint32_t arec_bytes;     // query tile: hi + lo operands + 128 x int4 lane info
+};
+
+__host__ __device__ inline FastShape fast_shape(int dim)
+{
+    FastShape s;
+    s.kp = (dim + 63) / 64 * 64;
+    s.nk = s.kp / 64;
+    s.btile_bytes = (uint32_t)s.nk * kFN * 128u;
+    s.rec_bytes = s.btile_bytes + 1024u + 32u;
+    s.atile_bytes = (uint32_t)s.nk * kFT * 128u;
+    s.arec_bytes = 2u * s.atile_bytes + 16u * kFT;
+    return s;
+}
+
+// Per-block and per-superblock summaries, placed after the block records.
+struct FastSummary {
+    float *cen, *c2, *rad;          // [nb][kp] centre, [nb] |c|^2, [nb] max |o - c|
+    int *ids;                       // [nb * kFB] slot -> object id (-1: padding)
+    int *pos;                       // [num] object id -> slot
+    float *sb_cen, *sb_c2, *sb_rad; // [nsb][kp], [nsb], [nsb]
+    int *sb_b0;                     // [nsb + 1] first block of each superblock
+};
+
+inline size_t fast_rec_region(const FastShape &fs, int nb)
+{
+    return ((size_t)nb * fs.rec_bytes + 255) & ~(size_t)255;
+}
+
+// Byte offsets of the summary arrays after the records, each 256-byte
+// aligned (the pruning kernels read centres as float4).
+struct FastSummaryOffsets {
+    size_t cen, c2, rad, ids, pos, sb_cen, sb_c2, sb_rad, sb_b0, end;
+};
+
+inline FastSummaryOffsets fast_summary_offsets(const FastShape &fs, int nb, int nsb, int n)
+{
+    FastSummaryOffsets o;
+    size_t off = fast_rec_region(fs, nb);
+    auto take = [&](size_t bytes) { size_t at = off; off += (bytes + 255) & ~(size_t)255; return at; };
+    o.cen = take(sizeof(float) * (size_t)nb * fs.kp);
+    o.c2 = take(sizeof(float) * (size_t)nb);
+    o.rad = take(sizeof(float) * (size_t)nb);
+    o.ids = take(sizeof(int) * (size_t)nb * kFB);
+    o.pos = take(sizeof(int) * (size_t)n);
+    o.sb_cen = take(sizeof(float) * (size_t)nsb * fs.kp);
+    o.sb_c2 = take(sizeof(float) * (size_t)nsb);
+    o.sb_rad = take(sizeof(float) * (size_t)nsb);
+    o.sb_b0 = take(sizeof(int) * ((size_t)nsb + 1));
+    o.end = off;
+    return o;
+}
+
+inline size_t fast_bytes(const FastShape &fs, int nb, int nsb, int n)
+{
+    return fast_summary_offsets(fs, nb, nsb, n).end;
+}
+
+inline FastSummary fast_summary(unsigned char *recs, const FastShape &fs, int nb, int nsb, int n)
+{
+    const FastSummaryOffsets o = fast_summary_offsets(fs, nb, nsb, n);
+    FastSummary s;
+    s.cen = (float *)(recs + o.cen);
+    s.c2 = (float *)(recs + o.c2);
+    s.rad = (float *)(recs + o.rad);
+    s.ids = (int *)(recs + o.ids);
+    s.pos = (int *)(recs + o.pos);
+    s.sb_cen = (float *)(recs + o.sb_cen);
+    s.sb_c2 = (float *)(recs + o.sb_c2);
+    s.sb_rad = (float *)(recs + o.sb_rad);
+    s.sb_b0 = (int *)(recs + o.sb_b0);
+    return s;
+}
+
+// Result of the order construction, in the index's scratch: positions of
+// the final order (perm: position -> object id), the blocks as position
+// ranges, and the superblock starts (sb_start[pos] = 1 where a superblock
+// begins).  Valid until the scratch is reused.
+struct FastOrder {
+    int nb = 0, nsb = 0;
+    const int *perm = nullptr;
+    const int *blk_l = nullptr, *blk_r = nullptr;   // [nb]
+    const int *blk_sb = nullptr;                    // [nb] superblock of each block
+    const int *sb_b0 = nullptr;                     // [nsb + 1]
+};
+
+// Build the filter's block order for the index's rows (L2).  Uses the
+// index's growable scratch; one host read-back per level.
+int fast_block_order(gts_index *idx, FastOrder *out, cudaStream_t st);
+
+}  // namespace gts

@@ -28,7 +28,7 @@ struct gts_index {
 
     // tensor-core filter (L2): per-block operand records, built on first use
     unsigned char *fast_recs = nullptr;
-    int fast_nb = 0;
+    int fast_nb = 0, fast_nsb = 0;   // filter blocks, superblocks
     int last_fast_overflow = 0;
     // device time of the filter kernel (CUDA events around each launch),
     // kept only while timing is on (gts_filter_timing)

@@ -53,3 +53,17 @@ def test_fast_falls_back_outside_its_shape(oracle):
         np.testing.assert_array_equal(kth, oracle.knn_brute(ds, q, 8)[0])
         kth = idx.knn(q, 100, form=gts.FORM_FAST)
         np.testing.assert_array_equal(kth, oracle.knn_brute(ds, q, 100)[0])
+
+
+def test_fast_batches_larger_than_one_run(oracle):
+    """More queries than one filter run holds (32,768) are answered in
+    consecutive runs over the same scratch; repeated query ids included."""
+    rows = G.gmm_rows(6000, 16, 12, 0.3, seed=11)
+    ds = oracle.Dataset(2, rows)
+    q = np.random.default_rng(12).integers(0, 6000, size=40000).astype(np.int32)
+    with gts.Index(rows, 2, max_h=4) as idx:
+        kth, ids, dis = idx.knn(q, 5, form=gts.FORM_FAST, return_ids=True)
+    bk, bi, bd = oracle.knn_brute(ds, q, 5)
+    np.testing.assert_array_equal(ids, bi)
+    np.testing.assert_array_equal(kth, bk)
+    np.testing.assert_array_equal(dis, bd)
