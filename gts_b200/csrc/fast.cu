@@ -55,6 +55,7 @@ using namespace sm100;
 constexpr int kFCand = 1024;          // candidate slots per query
 constexpr int kFItem = 16;            // blocks per filter work item
 constexpr int kFChunk = 64;           // balls tested per pruning step
+constexpr int kNeedBlkY = 8;          // block-pruning CTAs per tile
 constexpr int kFMaxBatch = 32768;     // queries per filter run (bounds the candidate lists)
 constexpr long long kFWait = 1ll << 22;   // bounded mbarrier polls (each at most 1 us)
 
@@ -401,6 +402,9 @@ __device__ __forceinline__ uint64_t need_chunk(const float *__restrict__ cen, co
     for (int i = 0; i < 8; i++)
 #pragma unroll
         for (int c = 0; c < 4; c++) acc[i][c] = 0.f;
+    // kp is a multiple of 64: unrolled so the shared loads of later j are in
+    // flight while the FMAs of earlier ones run
+#pragma unroll 4
     for (int j = 0; j < kp; j++) {
         const float4 qa = *reinterpret_cast<const float4 *>(Qs + j * kFT + tq * 4);
         const float4 qb = *reinterpret_cast<const float4 *>(Qs + j * kFT + 64 + tq * 4);
@@ -446,35 +450,53 @@ __device__ __forceinline__ uint64_t need_chunk(const float *__restrict__ cen, co
     return (uint64_t)sm.flags[0] | ((uint64_t)sm.flags[1] << 32);
 }
 
-// The blocks a tile needs.  Every CTA of the tile first tests all
-// superblocks (flags in shared memory), then CTA y takes every gridDim.y-th
-// needed superblock and tests its blocks; needed blocks are appended to
-// blist[tile][nbcap] (count in bcnt[tile]).
-__global__ void __launch_bounds__(256) k_need(const float *__restrict__ rows, const int *__restrict__ qids,
-                                              const unsigned char *__restrict__ arec, FastShape fs, int dim,
-                                              FastSummary bs, int nsb, const int *__restrict__ r2_bits,
-                                              int *__restrict__ blist, int *__restrict__ bcnt, int nbcap,
-                                              unsigned long long *stats)
+// Superblocks the tile needs: CTA (tile, y) tests superblock chunk y and
+// writes its two mask words sb_mask[tile][2y .. 2y+1].
+__global__ void __launch_bounds__(256) k_need_sb(const float *__restrict__ rows, const int *__restrict__ qids,
+                                                 const unsigned char *__restrict__ arec, FastShape fs, int dim,
+                                                 FastSummary bs, int nsb, const int *__restrict__ r2_bits,
+                                                 uint32_t *__restrict__ sb_mask, int nsbw)
 {
     extern __shared__ __align__(16) float nsm[];
     __shared__ NeedSmem sm;
     float *Qs = nsm, *Cs = nsm + fs.kp * kFT;
-    uint32_t *sbm = reinterpret_cast<uint32_t *>(Cs + fs.kp * kFChunk);
-    const int tile = blockIdx.x;
-    const int nsbw = (nsb + 31) / 32;
+    const int tile = blockIdx.x, ch = blockIdx.y;
     need_load_tile(rows, qids, arec, fs, dim, tile, r2_bits, Qs, sm);
-    for (int ch = 0; ch * kFChunk < nsb; ch++) {
-        const uint64_t m = need_chunk(bs.sb_cen, bs.sb_c2, bs.sb_rad, ch * kFChunk, nsb, fs.kp, Qs, Cs, sm);
-        if (threadIdx.x == 0) {
-            sbm[2 * ch] = (uint32_t)m;
-            if (2 * ch + 1 < nsbw) sbm[2 * ch + 1] = (uint32_t)(m >> 32);
-        }
+    const uint64_t m = need_chunk(bs.sb_cen, bs.sb_c2, bs.sb_rad, ch * kFChunk, nsb, fs.kp, Qs, Cs, sm);
+    if (threadIdx.x == 0) {
+        sb_mask[(size_t)tile * nsbw + 2 * ch] = (uint32_t)m;
+        if (2 * ch + 1 < nsbw) sb_mask[(size_t)tile * nsbw + 2 * ch + 1] = (uint32_t)(m >> 32);
     }
-    __syncthreads();
-    unsigned long long tested = 0;
-    int seen = 0;
+}
+
+// Blocks the tile needs, inside the superblocks it needs: CTA (tile, y)
+// takes every gridDim.y-th needed superblock; needed blocks are appended to
+// blist[tile][nbcap] (count in bcnt[tile]).
+__global__ void __launch_bounds__(256) k_need_blk(const float *__restrict__ rows, const int *__restrict__ qids,
+                                                  const unsigned char *__restrict__ arec, FastShape fs, int dim,
+                                                  FastSummary bs, const int *__restrict__ r2_bits,
+                                                  const uint32_t *__restrict__ sb_mask, int nsbw,
+                                                  int *__restrict__ blist, int *__restrict__ bcnt, int nbcap,
+                                                  unsigned long long *stats)
+{
+    extern __shared__ __align__(16) float nsm[];
+    __shared__ NeedSmem sm;
+    float *Qs = nsm, *Cs = nsm + fs.kp * kFT;
+    const int tile = blockIdx.x;
+    // the superblocks of this CTA first, so a CTA with none returns early
+    int mine = 0, seen = 0;
     for (int w = 0; w < nsbw; w++) {
-        uint32_t word = sbm[w];
+        const int c = __popc(sb_mask[(size_t)tile * nsbw + w]);
+        mine += (seen + c + (int)gridDim.y - 1 - (int)blockIdx.y) / (int)gridDim.y -
+                (seen + (int)gridDim.y - 1 - (int)blockIdx.y) / (int)gridDim.y;
+        seen += c;
+    }
+    if (mine == 0) return;
+    need_load_tile(rows, qids, arec, fs, dim, tile, r2_bits, Qs, sm);
+    unsigned long long tested = 0;
+    seen = 0;
+    for (int w = 0; w < nsbw; w++) {
+        uint32_t word = sb_mask[(size_t)tile * nsbw + w];
         while (word) {
             const int s = w * 32 + __ffs(word) - 1;
             word &= word - 1;
@@ -525,6 +547,7 @@ struct FastTileArgs {
     const int2 *items;           // (tile, first entry)
     const int *n_items;
     int nbcap, k;
+    int st_cap;                  // staged candidates per item (shared memory)
     FastShape fs;
     int *cand_pos;               // [qnum][kFCand] slots
     float *cand_lb, *cand_ub;    // [qnum][kFCand] bounds on d^2
@@ -538,7 +561,9 @@ struct FastTileArgs {
 constexpr int kFS = 3;         // block stages, each with its own TMEM accumulator
 constexpr int kFAccCols = 160; // TMEM columns between accumulators (kFN = 144 used)
 
-constexpr int kFStage = 512;   // candidates staged in shared memory per item
+// Candidates are staged in shared memory during an item; the capacity
+// (a.st_cap) is what the shared memory left after the operands holds.
+constexpr int kFStageMax = 4096;
 
 struct __align__(16) FastCtl {
     uint64_t full[kFS];    // block copy landed
@@ -549,15 +574,19 @@ struct __align__(16) FastCtl {
     int tile, nblk;
     int err;
     int blk[kFItem];       // the item's blocks
-    int st_n;              // staged candidates (may run past kFStage: the rest went straight out)
+    int st_n;              // staged candidates (may run past st_cap: the rest went straight out)
     int st_cnt[kFT];       // staged candidates per query lane; at the flush: their list offset
 };
 
-struct __align__(16) FastStaged {
-    int lane_rank;         // lane << 16 | rank within the lane, -1: unused entry
-    int slot;
-    float lb, ub;
+// 12 bytes: the slot (< 2^25) with the query lane in the top 7 bits
+// (all ones: an unused entry), the lower bound, and the lane rank with the
+// margin ub - lb as a half rounded up (so lb + margin >= ub).
+struct FastStaged {
+    uint32_t slot_lane;
+    float lb;
+    uint32_t rank_margin;
 };
+constexpr uint32_t kStagedUnused = 0xffffffffu;
 
 // Persistent filter kernel, one CTA per SM, 4 x CG epilogue warps + one
 // producer warp.  CG column groups: warps w, w+4, ... share TMEM lanes
@@ -588,9 +617,10 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
     const uint32_t arec_pad = (fs.arec_bytes + 1023u) & ~1023u;
     const uint32_t rec_pad = (fs.rec_bytes + 1023u) & ~1023u;
     unsigned char *B0 = base + arec_pad;
-    FastStaged *stg = reinterpret_cast<FastStaged *>(B0 + kFS * rec_pad);
-    float *heap = reinterpret_cast<float *>(stg + kFStage);
+    float *heap = reinterpret_cast<float *>(B0 + kFS * rec_pad);
     FastCtl &ctl = *reinterpret_cast<FastCtl *>(heap + NT * a.k);
+    FastStaged *stg = reinterpret_cast<FastStaged *>(&ctl + 1);
+    const int st_cap = a.st_cap;
 
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const bool producer = warp == NEW;
@@ -795,10 +825,10 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                     if (!np) continue;
                     appended += np;
                     int at = wbase + incl - np, rank = -1, gsl = 0;
-                    if (at + np <= kFStage) {
+                    if (at + np <= st_cap) {
                         rank = atomicAdd(&ctl.st_cnt[lq], np);
                     } else {
-                        for (int e = at; e < kFStage; e++) stg[e].lane_rank = -1;   // reserved, unused
+                        for (int e = at; e < st_cap; e++) stg[e].slot_lane = kStagedUnused;   // reserved, unused
                         gsl = atomicAdd(&a.cand_cnt[qi], np);
                     }
 #pragma unroll
@@ -810,7 +840,8 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                         const float ub = lb + 2.f * fmaf(A, dj, eb);
                         const int slot = blk * kFB + jj;
                         if (rank >= 0) {
-                            stg[at++] = FastStaged{(lq << 16) | rank, slot, lb, ub};
+                            const uint32_t mh = __half_as_ushort(__float2half_ru(ub - lb));
+                            stg[at++] = FastStaged{(uint32_t)slot | ((uint32_t)lq << 25), lb, (uint32_t)rank | (mh << 16)};
                             rank++;
                         } else {
                             if (gsl < kFCand) {
@@ -853,16 +884,17 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
             ctl.st_cnt[t] = (c > 0 && qi >= 0) ? atomicAdd(&a.cand_cnt[qi], c) : 0;
         }
         __syncthreads();
-        const int ns = min(ctl.st_n, kFStage);
+        const int ns = min(ctl.st_n, st_cap);
         for (int e = t; e < ns; e += NT + 32) {
             const FastStaged v = stg[e];
-            if (v.lane_rank < 0) continue;
-            const int l = v.lane_rank >> 16, qi = tinfo[l].x;
-            const int at = ctl.st_cnt[l] + (v.lane_rank & 0xffff);
+            if (v.slot_lane == kStagedUnused) continue;
+            const int l = (int)(v.slot_lane >> 25), qi = tinfo[l].x;
+            const int at = ctl.st_cnt[l] + (int)(v.rank_margin & 0xffffu);
             if (at < kFCand) {
-                a.cand_pos[(size_t)qi * kFCand + at] = v.slot;
+                const float margin = __half2float(__ushort_as_half((unsigned short)(v.rank_margin >> 16)));
+                a.cand_pos[(size_t)qi * kFCand + at] = (int)(v.slot_lane & 0x1ffffffu);
                 a.cand_lb[(size_t)qi * kFCand + at] = v.lb;
-                a.cand_ub[(size_t)qi * kFCand + at] = v.ub;
+                a.cand_ub[(size_t)qi * kFCand + at] = __fadd_ru(v.lb, margin);
             }
         }
         __syncthreads();
@@ -1069,10 +1101,21 @@ static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
 {
     const uint32_t arec_pad = (a.fs.arec_bytes + 1023u) & ~1023u;
     const uint32_t rec_pad = (a.fs.rec_bytes + 1023u) & ~1023u;
-    size_t smem = 1024 + (size_t)arec_pad + kFS * (size_t)rec_pad + sizeof(FastStaged) * kFStage +
-                  sizeof(float) * 128 * CG * (size_t)a.k + sizeof(FastCtl) + 64;
+    const size_t fixed = 1024 + (size_t)arec_pad + kFS * (size_t)rec_pad + sizeof(float) * 128 * CG * (size_t)a.k +
+                         sizeof(FastCtl) + 64;
+    int dev = 0, optin = 0;
+    GTS_CUDA_TRY(cudaGetDevice(&dev));
+    GTS_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    FastTileArgs b = a;
+    b.st_cap = (int)std::min<size_t>(kFStageMax, optin > (int)fixed ? ((size_t)optin - fixed) / sizeof(FastStaged) : 0);
+    b.st_cap &= ~31;
+    if (b.st_cap < 32) {
+        gts_set_error("tensor-core filter: %zu bytes of shared memory leave no room for candidate staging", fixed);
+        return GTS_ERR_INVALID;
+    }
+    const size_t smem = fixed + sizeof(FastStaged) * (size_t)b.st_cap;
     GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_tile<CG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_fast_tile<CG><<<grid, 128 * CG + 32, smem, st>>>(a);
+    k_fast_tile<CG><<<grid, 128 * CG + 32, smem, st>>>(b);
     GTS_CUDA_TRY(cudaGetLastError());
     return GTS_OK;
 }
@@ -1099,6 +1142,10 @@ static int fast_prepare(gts_index *idx, cudaStream_t st)
     int rc = fast_block_order(idx, &ord, st);
     if (rc) return rc;
     const int nb = ord.nb, nsb = ord.nsb;
+    if ((long long)nb * kFB >= (1ll << 25)) {   // staged candidates carry the slot in 25 bits
+        gts_set_error("tensor-core filter: %d blocks exceed the %d slots of the candidate format", nb, 1 << 25);
+        return GTS_ERR_INVALID;
+    }
     const size_t bytes = fast_bytes(fs, nb, nsb, idx->num);
     unsigned char *recs = nullptr;
     if ((rc = dev_alloc(&recs, bytes, nullptr))) return rc;
@@ -1127,6 +1174,7 @@ struct RunBufs {
     int *keys, *vals, *skeys, *order, *cpos, *ccnt, *r2, *ctr, *blist, *bcnt;
     float *clb, *cub_;
     unsigned char *arec;
+    uint32_t *sb_mask;
     int2 *items;
     void *cub;
     size_t cub_bytes;
@@ -1136,7 +1184,7 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
 {
     const FastShape fs = fast_shape(idx->dim);
     const int ntiles = (qnum + kFT - 1) / kFT;
-    const int nb = idx->fast_nb;
+    const int nb = idx->fast_nb, nsbw = (idx->fast_nsb + 31) / 32;
     const size_t itemcap = (size_t)ntiles * ((nb + kFItem - 1) / kFItem);
     size_t cub_bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (int *)nullptr, (int *)nullptr, (int *)nullptr,
@@ -1155,6 +1203,7 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
     r.r2 = (int *)take(4 * (size_t)qnum);
     r.ctr = (int *)take(8 * sizeof(int));   // failures, item counter, item count
     r.arec = take((size_t)ntiles * fs.arec_bytes);
+    r.sb_mask = (uint32_t *)take(4 * (size_t)ntiles * std::max(nsbw, 1));
     r.blist = (int *)take(4 * (size_t)ntiles * std::max(nb, 1));
     r.bcnt = (int *)take(4 * (size_t)ntiles);
     r.items = (int2 *)take(sizeof(int2) * std::max(itemcap, (size_t)1));
@@ -1201,12 +1250,13 @@ static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, 
     // the certified own-block seed; with a learned radius the smaller of the
     // two is used, and queries it under-predicts are answered again
     k_fast_seed<<<qnum, 128, 0, st>>>(idx->rows, d_qids, bs, idx->dim, k, r.r2);
-    const size_t need_smem = sizeof(float) * (size_t)fs.kp * (kFT + kFChunk) + sizeof(uint32_t) * (size_t)nsbw;
-    GTS_CUDA_TRY(cudaFuncSetAttribute(k_need, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
-    // several pruning CTAs per tile only when there are few tiles
-    const int ny = std::max(1, std::min(16, 2 * nsm / ntiles));
-    k_need<<<dim3(ntiles, ny), 256, need_smem, st>>>(idx->rows, d_qids, r.arec, fs, idx->dim, bs, nsb, r.r2, r.blist,
-                                                     r.bcnt, nb, idx->d_stats);
+    const size_t need_smem = sizeof(float) * (size_t)fs.kp * (kFT + kFChunk);
+    GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_sb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
+    GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
+    k_need_sb<<<dim3(ntiles, (nsb + kFChunk - 1) / kFChunk), 256, need_smem, st>>>(
+        idx->rows, d_qids, r.arec, fs, idx->dim, bs, nsb, r.r2, r.sb_mask, nsbw);
+    k_need_blk<<<dim3(ntiles, kNeedBlkY), 256, need_smem, st>>>(idx->rows, d_qids, r.arec, fs, idx->dim, bs, r.r2,
+                                                               r.sb_mask, nsbw, r.blist, r.bcnt, nb, idx->d_stats);
     k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, r.bcnt, nb, r.items, r.ctr + 2);
     GTS_CUDA_TRY(cudaGetLastError());
 
