@@ -81,7 +81,7 @@ class ClockSampler:
 
     def _read(self):
         for ln in self.proc.stdout:
-            self.lines.append(ln.strip())
+            self.lines.append((time.time(), ln.strip()))
 
     def __exit__(self, *exc):
         if self.proc:
@@ -91,10 +91,14 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, t0=None, t1=None):
+        """Median SM clock and the throttle reasons seen in [t0, t1] (host
+        wall-clock seconds; the whole sampling when None)."""
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ts, ln in self.lines:
+            if (t0 is not None and ts < t0) or (t1 is not None and ts > t1):
+                continue
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 8:
                 continue
@@ -243,6 +247,7 @@ def run_gts(args):
     def step():
         idx.knn_device(d_q.data_ptr(), Q, k, d_kth.data_ptr(), form=form, stream=stream.cuda_stream)
 
+    clocks = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -256,21 +261,36 @@ def run_gts(args):
         idx.filter_timing(reset=True)
     if args.profile:
         torch.cuda.profiler.start()
-    with ClockSampler(local) as clocks:
-        t_start = torch.cuda.Event(enable_timing=True)
-        t_end = torch.cuda.Event(enable_timing=True)
-        t_start.record(stream)
-        for i in range(args.steps):
-            ev[i][0].record(stream)
-            step()
-            ev[i][1].record(stream)
-        t_end.record(stream)
-        torch.cuda.synchronize()
+    launches0 = idx.kernel_launches()
+    wall0 = time.time()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        step()
+        ev[i][1].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    wall1 = time.time()
+    launches = idx.kernel_launches() - launches0
+    filter_ms, filter_launches = idx.filter_timing() if args.form == "fast" else (0.0, 0)
     if args.profile:
         torch.cuda.profiler.stop()
+    # nvidia-smi samples every 100 ms: when the timed steps are shorter than
+    # that, the same step keeps running (untimed) until 0.3 s have passed so
+    # the clock record covers this load
+    while time.time() - wall0 < 0.3:
+        step()
+        torch.cuda.synchronize()
+    wall2 = time.time()
+    time.sleep(0.15)   # let the last sample land
+    clocks.__exit__(None, None, None)
+    clock_summary = clocks.summary(wall0, wall2)
+    clock_summary["window_s"] = round(wall2 - wall0, 3)
+    clock_summary["timed_s"] = round(wall1 - wall0, 3)
     total_ms = t_start.elapsed_time(t_end)
     per_launch_ms = [a.elapsed_time(b) for a, b in ev]
-    filter_ms, filter_launches = idx.filter_timing() if args.form == "fast" else (0.0, 0)
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -302,20 +322,22 @@ def run_gts(args):
 
     peaks = measured_peaks_all()
     d = args.dim
-    # this library's kernels per step (CUB's radix-sort kernels not counted):
-    # plain: k_search; fast: k_fast_keys, k_fast_init, 2 x k_fast_tile,
-    # k_add_stat, k_fast_final, and k_search + 3 helpers when queries fall back
-    launches_per_step = 1 if args.form == "plain" else 6 + (4 if stats["fallback"] else 0)
     launch_ms = statistics.mean(per_launch_ms)
-    traffic = None
+    # DRAM traffic of the dominant kernel per launch: the ncu capture's bytes
+    # per unit (operand block for the filter, leaf object for the traversal)
+    # times the units this run processed per launch
+    per_unit = {}
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(f"{args.form}_k{k}_n{args.n}")
+            per_unit = json.load(f)
     if args.form == "plain":
         # every leaf row and pivot row a query reads, plus its own row and result
         alg_bytes = 4 * d * (stats["objects"] + stats["pivots"]) + Q * (4 * d + 8 * k)
         achieved = alg_bytes / (launch_ms / 1e3) / 1e9
+        traffic = None
+        if "k_search" in per_unit:
+            traffic = per_unit["k_search"]["dram_bytes_per_object"] * stats["objects"]
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                     "peak_kind": peaks["kind"], "kernel": "k_search",
@@ -333,25 +355,31 @@ def run_gts(args):
         flops = stats["blocks"] * 2 * 128 * 144 * kp * 2 / per_step
         kernel_ms = filter_ms / max(1, filter_launches)
         achieved = flops / (kernel_ms / 1e3) / 1e12
+        traffic = None
+        if "k_fast_tile" in per_unit:
+            traffic = per_unit["k_fast_tile"]["dram_bytes_per_block"] * stats["blocks"] / per_step
+        streamed = stats["bytes"] / per_step
         roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
                     "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"], "traffic": traffic,
                     "peak_kind": peaks["kind"], "kernel": "k_fast_tile",
                     "kernel_ms_per_launch": kernel_ms, "launches_per_step": per_step,
                     "kernel_share_of_step": filter_ms / total_ms,
                     "mma_flops_per_launch": flops,
-                    "streamed_bytes_per_launch": stats["bytes"] / per_step,
-                    "streamed_gbs": stats["bytes"] / per_step / (kernel_ms / 1e3) / 1e9,
+                    "streamed_bytes_per_launch": streamed,
+                    "streamed_gbs": streamed / (kernel_ms / 1e3) / 1e9,
+                    "streamed_hbm_frac": streamed / (kernel_ms / 1e3) / 1e9 / peaks["hbm_gbs"],
                     "per_query": {"blocks": stats["blocks"] / Q, "appended": stats["appended"] / Q,
                                   "exact_rechecks": stats["exact"] / Q,
                                   "fallback_queries": stats["fallback"], "passes": stats["passes"]},
                     "block_pairs_kept": (stats["blocks"] / stats["tested"]) if stats["tested"] else None}
     line = {"metric": "exact kNN queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/f64" if args.form == "plain" else "bf16/f32/f64",
             "data": "synthetic (seeded Gaussian mixture; the paper's data sets are absent)",
             "config": config_dict(args, world), "build_s": build_s, "learned_radius": learn,
             "roofline": roofline,
-            "e2e": e2e, "gpu_launches": args.steps * launches_per_step, "clocks": clocks.summary()}
+            "e2e": e2e, "gpu_launches": launches, "clocks": clock_summary}
     if rank == 0 and world == 1 and args.cpu_sample > 0:
         line["cpu_baseline"] = cpu_baseline(rows, qids, k, args.cpu_sample, kth_gpu)
     if rank == 0:

@@ -271,6 +271,12 @@ class Index:
         _check(self._lib.gts_filter_timing(self._h, 1 if reset else 0, C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
+    def kernel_launches(self) -> int:
+        """Kernels this library launched for searches on this handle so far."""
+        n = C.c_longlong()
+        _check(self._lib.gts_kernel_launches(self._h, C.byref(n)))
+        return n.value
+
     def knn(self, qids, k: int, form: int = FORM_PLAIN, return_ids: bool = False):
         q = np.ascontiguousarray(qids, dtype=np.int32)
         kth = np.empty(len(q), np.float32)

@@ -415,6 +415,16 @@ extern "C" int gts_filter_timing(gts_index *idx, int reset, double *ms, long lon
     return GTS_OK;
 }
 
+extern "C" int gts_kernel_launches(const gts_index *idx, long long *count)
+{
+    if (!idx || !count) {
+        gts_set_error("null argument");
+        return GTS_ERR_INVALID;
+    }
+    *count = idx->kernel_launches;
+    return GTS_OK;
+}
+
 extern "C" int gts_index_set_stream(gts_index *idx, void *stream)
 {
     if (!idx) {

@@ -1240,24 +1240,31 @@ static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, 
     const FastSummary bs = fast_summary(idx->fast_recs, fs, nb, nsb, idx->num);
 
     k_fast_keys<<<(qnum + 255) / 256, 256, 0, st>>>(d_qids, qnum, bs.pos, r.keys, r.vals);
+    idx->kernel_launches++;
     size_t cb = r.cub_bytes;
     GTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(r.cub, cb, r.keys, r.skeys, r.vals, r.order, qnum, 0, 32, st));
     k_fast_init<<<(qnum + 255) / 256, 256, 0, st>>>(qnum, r.ccnt, r.r2, carry);
+    idx->kernel_launches++;
     if (learned && (rc = mlp_seed(idx, d_qids, qnum, k, r.r2, st))) return rc;
     GTS_CUDA_TRY(cudaMemsetAsync(r.ctr, 0, 8 * sizeof(int), st));
     GTS_CUDA_TRY(cudaMemsetAsync(r.bcnt, 0, sizeof(int) * ntiles, st));
     k_fast_arec<<<ntiles, 128, 0, st>>>(idx->rows, d_qids, r.order, qnum, idx->dim, fs, r.arec);
+    idx->kernel_launches++;
     // the certified own-block seed; with a learned radius the smaller of the
     // two is used, and queries it under-predicts are answered again
     k_fast_seed<<<qnum, 128, 0, st>>>(idx->rows, d_qids, bs, idx->dim, k, r.r2);
+    idx->kernel_launches++;
     const size_t need_smem = sizeof(float) * (size_t)fs.kp * (kFT + kFChunk);
     GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_sb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
     GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
     k_need_sb<<<dim3(ntiles, (nsb + kFChunk - 1) / kFChunk), 256, need_smem, st>>>(
         idx->rows, d_qids, r.arec, fs, idx->dim, bs, nsb, r.r2, r.sb_mask, nsbw);
+    idx->kernel_launches++;
     k_need_blk<<<dim3(ntiles, kNeedBlkY), 256, need_smem, st>>>(idx->rows, d_qids, r.arec, fs, idx->dim, bs, r.r2,
                                                                r.sb_mask, nsbw, r.blist, r.bcnt, nb, idx->d_stats);
+    idx->kernel_launches++;
     k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, r.bcnt, nb, r.items, r.ctr + 2);
+    idx->kernel_launches++;
     GTS_CUDA_TRY(cudaGetLastError());
 
     FastTileArgs a;
@@ -1281,11 +1288,14 @@ static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, 
     const bool timed = idx->time_filter && idx->fev[0];
     if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[0], st));
     if ((rc = launch_fast_tile(a, nsm, st))) return rc;
+    idx->kernel_launches++;
     if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[1], st));
     k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 1ull);
+    idx->kernel_launches++;
     k_fast_final<<<qnum, 128, 0, st>>>(idx->rows, idx->dim, idx->num, bs.ids, nb * kFB, d_qids, k,
                                         idx->params.infi_dis, r.cpos, r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids,
                                         d_dists, d_fail, r.ctr, idx->d_stats);
+    idx->kernel_launches++;
     GTS_CUDA_TRY(cudaGetLastError());
     int status = 0;
     GTS_CUDA_TRY(cudaMemcpyAsync(&status, idx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1345,7 +1355,9 @@ static int rerun_failed(gts_index *idx, FastCall &fc, int stage, const int *pare
     int *sub_ids = d_ids ? b.sub_ids : nullptr;
     float *sub_dis = d_dists ? b.sub_dis : nullptr;
     k_gather_i<<<(n + 255) / 256, 256, 0, st>>>(parent_q, b.fail, n, b.sub_q);
+    idx->kernel_launches++;
     if (stage == 1 && r2_prev) k_gather_i<<<(n + 255) / 256, 256, 0, st>>>(r2_prev, b.fail, n, b.sub_r2);
+    idx->kernel_launches++;
     int rc;
     if (stage < 2) {
         int n2 = 0, *r2 = nullptr;
@@ -1357,6 +1369,7 @@ static int rerun_failed(gts_index *idx, FastCall &fc, int stage, const int *pare
             return rc;
     } else {
         k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 4, (unsigned long long)n);
+        idx->kernel_launches++;
         idx->keep_stats = true;
         rc = search_knn(idx, b.sub_q, n, k, 0, b.sub_kth, sub_ids, sub_dis, st);
         idx->keep_stats = false;
@@ -1364,6 +1377,7 @@ static int rerun_failed(gts_index *idx, FastCall &fc, int stage, const int *pare
     }
     k_scatter_results<<<(n + 255) / 256, 256, 0, st>>>(b.fail, n, k, b.sub_kth, sub_ids, sub_dis, d_kth, d_ids,
                                                        d_dists);
+    idx->kernel_launches++;
     GTS_CUDA_TRY(cudaGetLastError());
     return GTS_OK;
 }
@@ -1440,13 +1454,16 @@ int search_knn_fast_fixed(gts_index *idx, const int *d_qids, int qnum, int k, fl
     int *sub_ids = d_ids ? b.sub_ids : nullptr;
     float *sub_dis = d_dists ? b.sub_dis : nullptr;
     k_gather_i<<<(n_fail + 255) / 256, 256, 0, st>>>(d_qids, b.fail, n_fail, b.sub_q);
+    idx->kernel_launches++;
     k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 4, (unsigned long long)n_fail);
+    idx->kernel_launches++;
     idx->keep_stats = true;
     rc = search_knn(idx, b.sub_q, n_fail, k, 0, b.sub_kth, sub_ids, sub_dis, st);
     idx->keep_stats = false;
     if (rc) return rc;
     k_scatter_results<<<(n_fail + 255) / 256, 256, 0, st>>>(b.fail, n_fail, k, b.sub_kth, sub_ids, sub_dis, d_kth,
                                                            d_ids, d_dists);
+    idx->kernel_launches++;
     GTS_CUDA_TRY(cudaGetLastError());
     GTS_CUDA_TRY(cudaStreamSynchronize(st));
     return GTS_OK;

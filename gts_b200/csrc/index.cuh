@@ -36,6 +36,8 @@ struct gts_index {
     cudaEvent_t fev[2] = {nullptr, nullptr};
     double filter_ms = 0.0;
     long long filter_launches = 0;
+    // kernels this library launched for searches on this handle (host count)
+    long long kernel_launches = 0;
 
     // reusable per-call scratch (grown on demand, freed with the handle)
     void *scratch = nullptr;

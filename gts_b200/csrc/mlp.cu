@@ -307,6 +307,7 @@ int mlp_seed(gts_index *idx, const int *d_qids, int qnum, int k, int *d_r2_bits,
     k_mlp_infer<<<(qnum + kInferQ - 1) / kInferQ, kMH, 0, st>>>(
         idx->rows, idx->dim, d_qids, qnum, idx->mlp_piv, idx->mlp_npiv, k, idx->mlp_P, idx->mlp_norm,
         idx->mlp_norm + kMIn, idx->mlp_ymu, idx->mlp_ysig, idx->mlp_widen, d_r2_bits);
+    idx->kernel_launches++;
     GTS_CUDA_TRY(cudaGetLastError());
     return GTS_OK;
 }

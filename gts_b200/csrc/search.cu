@@ -553,6 +553,7 @@ static int run_search(gts_index *idx, SearchArgs &a, cudaStream_t st)
     int grid = nsm * per_sm;
     if (grid > a.qnum) grid = a.qnum;
     k_search<<<grid, kThreads, smem, st>>>(a);
+    idx->kernel_launches++;
     GTS_CUDA_TRY(cudaGetLastError());
     int status = 0;
     GTS_CUDA_TRY(cudaMemcpyAsync(&status, idx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -128,6 +128,10 @@ int gts_search_stats(const gts_index *idx, unsigned long long *out8);
  * *ms / *launches (nullable) receive the totals since the last reset. */
 int gts_filter_timing(gts_index *idx, int reset, double *ms, long long *launches);
 
+/* No counterpart in the reference.  Number of kernels this library has
+ * launched for searches on this handle (a host-side count, cumulative). */
+int gts_kernel_launches(const gts_index *idx, long long *count);
+
 /* ---------------------------------------------------------------- search */
 
 /* searchIndexKnnV2 (search_v2.cuh:975-1228) -> res_dis.
