@@ -129,7 +129,8 @@ def config_dict(args, world):
             "k": args.k, "tree_order": 10, "max_size": 20, "max_h": args.max_h,
             "form": args.form + ("" if args.form == "plain" else
                                  (" (block-pruned bf16 filter)" if args.no_learn else
-                                  " (learned radius + block-pruned bf16 filter)")),
+                                  " (learned radius trained + block-pruned bf16 filter; the autotuner "
+                                  "decides per k whether the learned seed is used)")),
             "parallelism": f"query-sharded replicas x{world}",
             "l2_flush": "no (512 MB data set > 126 MB L2)"}
 
@@ -378,6 +379,7 @@ def run_gts(args):
             "dtype": "f32/f64" if args.form == "plain" else "bf16/f32/f64",
             "data": "synthetic (seeded Gaussian mixture; the paper's data sets are absent)",
             "config": config_dict(args, world), "build_s": build_s, "learned_radius": learn,
+            "autotune": idx.fast_config(k) if args.form == "fast" else None,
             "roofline": roofline,
             "e2e": e2e, "gpu_launches": launches, "clocks": clock_summary}
     if rank == 0 and world == 1 and args.cpu_sample > 0:

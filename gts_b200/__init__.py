@@ -271,6 +271,16 @@ class Index:
         _check(self._lib.gts_filter_timing(self._h, 1 if reset else 0, C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
+    def fast_config(self, k: int) -> dict:
+        """The autotuned (or default) fast-form configuration for k."""
+        v = [C.c_int() for _ in range(4)]
+        _check(self._lib.gts_fast_config(self._h, k, *[C.byref(x) for x in v]))
+        return {"tuned": bool(v[0].value), "learned_seed": bool(v[1].value), "col_groups": v[2].value,
+                "item_blocks": v[3].value}
+
+    def fast_autotune_reset(self):
+        _check(self._lib.gts_fast_autotune_reset(self._h))
+
     def kernel_launches(self) -> int:
         """Kernels this library launched for searches on this handle so far."""
         n = C.c_longlong()

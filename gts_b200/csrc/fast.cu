@@ -24,7 +24,7 @@
 //    some query of the tile can reach.  Blocks no query of the tile can
 //    reach within its seed are never copied or multiplied (GTS's pivot
 //    pruning, done with balls instead of rings).  The needed blocks of a
-//    tile become work items of up to kFItem blocks.
+//    tile become work items of up to 8-32 blocks (autotuned).
 //  * filter: a persistent CTA per SM takes work items.  One producer warp
 //    streams the tile's query operand and the item's block records with
 //    bulk copies and issues a 128 x 144 x K MMA chain per block into one of
@@ -53,7 +53,8 @@ namespace gts {
 using namespace sm100;
 
 constexpr int kFCand = 1024;          // candidate slots per query
-constexpr int kFItem = 16;            // blocks per filter work item
+constexpr int kFItemMax = 32;         // blocks per filter work item at most (autotuned: 8, 16 or 32)
+constexpr int kFItemMin = 8;
 constexpr int kFChunk = 64;           // balls tested per pruning step
 constexpr int kNeedBlkY = 8;          // block-pruning CTAs per tile
 constexpr int kFMaxBatch = 32768;     // queries per filter run (bounds the candidate lists)
@@ -524,17 +525,17 @@ __global__ void __launch_bounds__(256) k_need_blk(const float *__restrict__ rows
     if (threadIdx.x == 0 && stats && tested) atomicAdd(&stats[7], tested);
 }
 
-// Work items: (tile, first list entry) per kFItem needed blocks of a tile.
-__global__ void k_items(int ntiles, const int *__restrict__ bcnt, int nbcap, int2 *__restrict__ items,
+// Work items: (tile, first list entry) per `item` needed blocks of a tile.
+__global__ void k_items(int ntiles, const int *__restrict__ bcnt, int nbcap, int item, int2 *__restrict__ items,
                         int *__restrict__ n_items)
 {
     const int tile = blockIdx.x * blockDim.x + threadIdx.x;
     if (tile >= ntiles) return;
     const int cnt = min(bcnt[tile], nbcap);
-    const int nit = (cnt + kFItem - 1) / kFItem;
+    const int nit = (cnt + item - 1) / item;
     if (nit == 0) return;
     const int base = atomicAdd(n_items, nit);
-    for (int i = 0; i < nit; i++) items[base + i] = make_int2(tile, i * kFItem);
+    for (int i = 0; i < nit; i++) items[base + i] = make_int2(tile, i * item);
 }
 
 // ---------------------------------------------------------------- filter
@@ -547,6 +548,7 @@ struct FastTileArgs {
     const int2 *items;           // (tile, first entry)
     const int *n_items;
     int nbcap, k;
+    int item;                    // blocks per work item (<= kFItemMax)
     int st_cap;                  // staged candidates per item (shared memory)
     FastShape fs;
     int *cand_pos;               // [qnum][kFCand] slots
@@ -573,7 +575,7 @@ struct __align__(16) FastCtl {
     uint32_t tmem;
     int tile, nblk;
     int err;
-    int blk[kFItem];       // the item's blocks
+    int blk[kFItemMax];    // the item's blocks
     int st_n;              // staged candidates (may run past st_cap: the rest went straight out)
     int st_cnt[kFT];       // staged candidates per query lane; at the flush: their list offset
 };
@@ -592,7 +594,7 @@ constexpr uint32_t kStagedUnused = 0xffffffffu;
 // producer warp.  CG column groups: warps w, w+4, ... share TMEM lanes
 // 32*(w%4)..+31 (the same 32 queries) and split the 128 object columns.
 //
-// Per item (a tile and up to kFItem of its needed blocks), with gi counting
+// Per item (a tile and up to a.item of its needed blocks), with gi counting
 // blocks over the CTA's life (barrier phases follow it):
 //   producer:  copy A; copy blocks 0..2 into stages gi%3; for each block:
 //              wait its copy, wait the epilogue of block gi-2 (frees TMEM
@@ -662,7 +664,7 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
             if (it < *a.n_items) {
                 const int2 e = a.items[it];
                 tile = e.x;
-                nblk = min(kFItem, min(a.bcnt[tile], a.nbcap) - e.y);
+                nblk = min(a.item, min(a.bcnt[tile], a.nbcap) - e.y);
                 for (int j = 0; j < nblk; j++) ctl.blk[j] = a.blist[(size_t)tile * a.nbcap + e.y + j];
             }
             ctl.tile = tile;
@@ -1096,6 +1098,23 @@ __global__ void k_scatter_results(const int *idx, int n, int k, const float *kth
 // (threads x k floats, at most 32 KB of shared memory) allow.
 static int fast_cg(int k) { return k <= 16 ? 4 : (k <= 32 ? 2 : 1); }
 
+// One configuration of the fast form: seed with the learned radius or not,
+// epilogue column groups (warps per query lane), blocks per work item.
+struct FastCfg {
+    bool learned;
+    int cg, item;
+};
+
+static int cfg_pack(const FastCfg &c) { return 1 | (c.learned ? 2 : 0) | (c.cg << 2) | (c.item << 8); }
+static FastCfg cfg_unpack(int v) { return FastCfg{(v & 2) != 0, (v >> 2) & 7, (v >> 8) & 63}; }
+
+static FastCfg fast_default_cfg(const gts_index *idx, int k)
+{
+    // measured on clustered data: the own-block seed is tight for small k,
+    // the learned radius pays for its re-answers from k = 16 on
+    return FastCfg{idx->mlp_ready && k >= 16, fast_cg(k), 16};
+}
+
 template <int CG>
 static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
 {
@@ -1120,9 +1139,9 @@ static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
     return GTS_OK;
 }
 
-static int launch_fast_tile(const FastTileArgs &a, int grid, cudaStream_t st)
+static int launch_fast_tile(const FastTileArgs &a, int cg, int grid, cudaStream_t st)
 {
-    switch (fast_cg(a.k)) {
+    switch (cg) {
     case 4: return launch_fast_tile_cg<4>(a, grid, st);
     case 2: return launch_fast_tile_cg<2>(a, grid, st);
     default: return launch_fast_tile_cg<1>(a, grid, st);
@@ -1185,7 +1204,7 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
     const FastShape fs = fast_shape(idx->dim);
     const int ntiles = (qnum + kFT - 1) / kFT;
     const int nb = idx->fast_nb, nsbw = (idx->fast_nsb + 31) / 32;
-    const size_t itemcap = (size_t)ntiles * ((nb + kFItem - 1) / kFItem);
+    const size_t itemcap = (size_t)ntiles * ((nb + kFItemMin - 1) / kFItemMin);
     size_t cub_bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (int *)nullptr, (int *)nullptr, (int *)nullptr,
                                     (int *)nullptr, qnum, 0, 32, (cudaStream_t)0);
@@ -1221,8 +1240,8 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
 // bounds (valid until the region is reused).  region: scratch of at least
 // plan_run(qnum) bytes.
 static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, const int *d_qids, int qnum, int k,
-                    bool learned, const int *carry, float *d_kth, int *d_ids, float *d_dists, int *d_fail,
-                    int *n_fail, int **r2_out, cudaStream_t st)
+                    const FastCfg &cfg, bool learned, const int *carry, float *d_kth, int *d_ids, float *d_dists,
+                    int *d_fail, int *n_fail, int **r2_out, cudaStream_t st)
 {
     const FastShape fs = fast_shape(idx->dim);
     const int ntiles = (qnum + kFT - 1) / kFT;
@@ -1263,7 +1282,7 @@ static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, 
     k_need_blk<<<dim3(ntiles, kNeedBlkY), 256, need_smem, st>>>(idx->rows, d_qids, r.arec, fs, idx->dim, bs, r.r2,
                                                                r.sb_mask, nsbw, r.blist, r.bcnt, nb, idx->d_stats);
     idx->kernel_launches++;
-    k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, r.bcnt, nb, r.items, r.ctr + 2);
+    k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, r.bcnt, nb, cfg.item, r.items, r.ctr + 2);
     idx->kernel_launches++;
     GTS_CUDA_TRY(cudaGetLastError());
 
@@ -1276,6 +1295,7 @@ static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, 
     a.n_items = r.ctr + 2;
     a.nbcap = nb;
     a.k = k;
+    a.item = cfg.item;
     a.fs = fs;
     a.cand_pos = r.cpos;
     a.cand_lb = r.clb;
@@ -1287,7 +1307,7 @@ static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, 
     a.stats = idx->d_stats;
     const bool timed = idx->time_filter && idx->fev[0];
     if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[0], st));
-    if ((rc = launch_fast_tile(a, nsm, st))) return rc;
+    if ((rc = launch_fast_tile(a, cfg.cg, nsm, st))) return rc;
     idx->kernel_launches++;
     if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[1], st));
     k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 1ull);
@@ -1348,24 +1368,27 @@ struct FastCall {
 // 1 -> after a run from certified seeds (its list overflowed): the filter
 //      again, starting from the bound that run reached (r2_prev);
 // 2 -> the plain traversal.
-static int rerun_failed(gts_index *idx, FastCall &fc, int stage, const int *parent_q, int n, const int *r2_prev,
-                        int k, float *d_kth, int *d_ids, float *d_dists, cudaStream_t st)
+static int rerun_failed(gts_index *idx, FastCall &fc, const FastCfg &cfg, int stage, const int *parent_q, int n,
+                        const int *r2_prev, int k, float *d_kth, int *d_ids, float *d_dists, cudaStream_t st)
 {
     Book &b = fc.book[stage];
     int *sub_ids = d_ids ? b.sub_ids : nullptr;
     float *sub_dis = d_dists ? b.sub_dis : nullptr;
     k_gather_i<<<(n + 255) / 256, 256, 0, st>>>(parent_q, b.fail, n, b.sub_q);
     idx->kernel_launches++;
-    if (stage == 1 && r2_prev) k_gather_i<<<(n + 255) / 256, 256, 0, st>>>(r2_prev, b.fail, n, b.sub_r2);
-    idx->kernel_launches++;
+    if (stage == 1 && r2_prev) {
+        k_gather_i<<<(n + 255) / 256, 256, 0, st>>>(r2_prev, b.fail, n, b.sub_r2);
+        idx->kernel_launches++;
+    }
     int rc;
     if (stage < 2) {
         int n2 = 0, *r2 = nullptr;
-        if ((rc = fast_run(idx, fc.region, fc.region_bytes, b.sub_q, n, k, false,
+        if ((rc = fast_run(idx, fc.region, fc.region_bytes, b.sub_q, n, k, cfg, false,
                            stage == 1 && r2_prev ? b.sub_r2 : nullptr, b.sub_kth, sub_ids, sub_dis,
                            fc.book[stage + 1].fail, &n2, &r2, st)))
             return rc;
-        if (n2 > 0 && (rc = rerun_failed(idx, fc, stage + 1, b.sub_q, n2, r2, k, b.sub_kth, sub_ids, sub_dis, st)))
+        if (n2 > 0 &&
+            (rc = rerun_failed(idx, fc, cfg, stage + 1, b.sub_q, n2, r2, k, b.sub_kth, sub_ids, sub_dis, st)))
             return rc;
     } else {
         k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 4, (unsigned long long)n);
@@ -1382,14 +1405,86 @@ static int rerun_failed(gts_index *idx, FastCall &fc, int stage, const int *pare
     return GTS_OK;
 }
 
+// The whole batch with one configuration: filter runs of at most qc
+// queries, each followed by the re-answer stages its failures need.
+static int fast_search_cfg(gts_index *idx, FastCall &fc, int qc, const FastCfg &cfg, const int *d_qids, int qnum,
+                           int k, float *d_kth, int *d_ids, float *d_dists, cudaStream_t st)
+{
+    GTS_CUDA_TRY(cudaMemsetAsync(idx->d_status, 0, sizeof(int), st));
+    GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, kStatsN * sizeof(unsigned long long), st));
+    const bool learned = cfg.learned && idx->mlp_ready;
+    const int first = learned ? 0 : 1;
+    int total_fail = 0, rc;
+    for (int q0 = 0; q0 < qnum; q0 += qc) {
+        const int qn = std::min(qc, qnum - q0);
+        int n_fail = 0, *r2 = nullptr;
+        float *kth = d_kth + q0;
+        int *ids = d_ids ? d_ids + (size_t)q0 * k : nullptr;
+        float *dis = d_dists ? d_dists + (size_t)q0 * k : nullptr;
+        if ((rc = fast_run(idx, fc.region, fc.region_bytes, d_qids + q0, qn, k, cfg, learned, nullptr, kth, ids,
+                           dis, fc.book[first].fail, &n_fail, &r2, st)))
+            return rc;
+        total_fail += n_fail;
+        if (n_fail > 0 && (rc = rerun_failed(idx, fc, cfg, first, d_qids + q0, n_fail, r2, k, kth, ids, dis, st)))
+            return rc;
+    }
+    idx->last_fast_overflow = total_fail;
+    GTS_CUDA_TRY(cudaStreamSynchronize(st));
+    return GTS_OK;
+}
+
+// Autotuner.  The first batch of at least kTuneMinQueries queries with a
+// given k runs once per candidate configuration (learned seed on / off when
+// a model is trained, 4 / 2 / 1 epilogue column groups as the heap fits, 8 /
+// 16 / 32 blocks per work item), timed with CUDA events; every candidate
+// returns the same exact answers, so the fastest is kept for this k and
+// index (until the index is rebuilt or the model retrained).  Smaller batches
+// use the default configuration without tuning.
+constexpr int kTuneMinQueries = 2048;
+
+static int fast_autotune(gts_index *idx, FastCall &fc, int qc, const int *d_qids, int qnum, int k, float *d_kth,
+                         int *d_ids, float *d_dists, cudaStream_t st, FastCfg *best_out)
+{
+    cudaEvent_t e0, e1;
+    GTS_CUDA_TRY(cudaEventCreate(&e0));
+    GTS_CUDA_TRY(cudaEventCreate(&e1));
+    FastCfg best = fast_default_cfg(idx, k);
+    float best_ms = 3.0e38f;
+    int rc = GTS_OK;
+    for (int learned = 0; learned <= (idx->mlp_ready ? 1 : 0) && rc == GTS_OK; learned++)
+        for (int cg = 4; cg >= 1 && rc == GTS_OK; cg >>= 1) {
+            if (cg * k > 64) continue;   // heaps: 128 cg threads x k floats <= 32 KB
+            for (int item = 8; item <= kFItemMax && rc == GTS_OK; item *= 2) {
+                const FastCfg c{learned != 0, cg, item};
+                if ((rc = (int)cudaEventRecord(e0, st)) != 0) {
+                    rc = GTS_ERR_CUDA;
+                    break;
+                }
+                if ((rc = fast_search_cfg(idx, fc, qc, c, d_qids, qnum, k, d_kth, d_ids, d_dists, st))) break;
+                float ms = 0.f;
+                if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                    cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+                    rc = GTS_ERR_CUDA;
+                    break;
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = c;
+                }
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc == GTS_ERR_CUDA) gts_set_error("autotune: CUDA event failed");
+    *best_out = best;
+    return rc;
+}
+
 int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                     float *d_dists, cudaStream_t st)
 {
     int rc = fast_prepare(idx, st);
     if (rc) return rc;
-    GTS_CUDA_TRY(cudaMemsetAsync(idx->d_status, 0, sizeof(int), st));
-    GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, kStatsN * sizeof(unsigned long long), st));
-    const bool learned = idx->mlp_ready;
     // one scratch region for a batch of at most kFMaxBatch queries, reused
     // by the re-answer stages, plus their bookkeeping
     const int qc = std::min(qnum, kFMaxBatch);
@@ -1400,24 +1495,16 @@ int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d
     fc.region = (unsigned char *)idx->scratch;
     fc.region_bytes = rbytes;
     for (int s = 0; s < 3; s++) plan_book(qc, k, fc.region + rbytes + s * bbytes, &fc.book[s]);
-    const int first = learned ? 0 : 1;
-    int total_fail = 0;
-    for (int q0 = 0; q0 < qnum; q0 += qc) {
-        const int qn = std::min(qc, qnum - q0);
-        int n_fail = 0, *r2 = nullptr;
-        float *kth = d_kth + q0;
-        int *ids = d_ids ? d_ids + (size_t)q0 * k : nullptr;
-        float *dis = d_dists ? d_dists + (size_t)q0 * k : nullptr;
-        if ((rc = fast_run(idx, fc.region, rbytes, d_qids + q0, qn, k, learned, nullptr, kth, ids, dis,
-                           fc.book[first].fail, &n_fail, &r2, st)))
-            return rc;
-        total_fail += n_fail;
-        if (n_fail > 0 && (rc = rerun_failed(idx, fc, first, d_qids + q0, n_fail, r2, k, kth, ids, dis, st)))
-            return rc;
+    FastCfg cfg;
+    if (idx->fast_cfg[k]) {
+        cfg = cfg_unpack(idx->fast_cfg[k]);
+    } else if (qnum >= kTuneMinQueries) {
+        if ((rc = fast_autotune(idx, fc, qc, d_qids, qnum, k, d_kth, d_ids, d_dists, st, &cfg))) return rc;
+        idx->fast_cfg[k] = cfg_pack(cfg);
+    } else {
+        cfg = fast_default_cfg(idx, k);
     }
-    idx->last_fast_overflow = total_fail;
-    GTS_CUDA_TRY(cudaStreamSynchronize(st));
-    return GTS_OK;
+    return fast_search_cfg(idx, fc, qc, cfg, d_qids, qnum, k, d_kth, d_ids, d_dists, st);
 }
 
 // The filter without the learned seed, with every buffer carved out of
@@ -1446,7 +1533,8 @@ int search_knn_fast_fixed(gts_index *idx, const int *d_qids, int qnum, int k, fl
     GTS_CUDA_TRY(cudaMemsetAsync(idx->d_status, 0, sizeof(int), st));
     GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, kStatsN * sizeof(unsigned long long), st));
     int n_fail = 0, rc;
-    if ((rc = fast_run(idx, scratch + bbytes, bytes - bbytes, d_qids, qnum, k, false, nullptr, d_kth, d_ids, d_dists,
+    const FastCfg cfg{false, fast_cg(k), 16};
+    if ((rc = fast_run(idx, scratch + bbytes, bytes - bbytes, d_qids, qnum, k, cfg, false, nullptr, d_kth, d_ids, d_dists,
                        b.fail, &n_fail, nullptr, st)))
         return rc;
     idx->last_fast_overflow = n_fail;
@@ -1469,4 +1557,38 @@ int search_knn_fast_fixed(gts_index *idx, const int *d_qids, int qnum, int k, fl
     return GTS_OK;
 }
 
+int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *cg, int *item)
+{
+    if (k < 1 || k > kFMaxK) {
+        gts_set_error("k must be in [1, %d], got %d", kFMaxK, k);
+        return GTS_ERR_INVALID;
+    }
+    const int v = idx->fast_cfg[k];
+    const FastCfg c = v ? cfg_unpack(v) : fast_default_cfg(idx, k);
+    if (tuned) *tuned = v ? 1 : 0;
+    if (learned) *learned = c.learned ? 1 : 0;
+    if (cg) *cg = c.cg;
+    if (item) *item = c.item;
+    return GTS_OK;
+}
+
 }  // namespace gts
+
+extern "C" int gts_fast_config(const gts_index *idx, int k, int *tuned, int *learned, int *col_groups, int *item_blocks)
+{
+    if (!idx) {
+        gts_set_error("null index");
+        return GTS_ERR_INVALID;
+    }
+    return gts::fast_config_get(idx, k, tuned, learned, col_groups, item_blocks);
+}
+
+extern "C" int gts_fast_autotune_reset(gts_index *idx)
+{
+    if (!idx) {
+        gts_set_error("null index");
+        return GTS_ERR_INVALID;
+    }
+    for (int &c : idx->fast_cfg) c = 0;
+    return GTS_OK;
+}

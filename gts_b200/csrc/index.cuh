@@ -38,6 +38,9 @@ struct gts_index {
     long long filter_launches = 0;
     // kernels this library launched for searches on this handle (host count)
     long long kernel_launches = 0;
+    // autotuned fast-form configuration per k (fast.cu): 0 = not tuned, else
+    // 1 | learned << 1 | column groups << 2 | blocks per item << 8
+    int fast_cfg[65] = {};
 
     // reusable per-call scratch (grown on demand, freed with the handle)
     void *scratch = nullptr;
@@ -88,6 +91,7 @@ bool fast_supported(const gts_index *idx, int k);
 int mlp_seed(gts_index *idx, const int *d_qids, int qnum, int k, int *d_r2_bits, cudaStream_t st);
 int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                     float *d_dists, cudaStream_t s);
+int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *cg, int *item);
 // Unseeded filter with all scratch inside the caller's fixed buffer.
 int search_knn_fast_fixed(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                           float *d_dists, unsigned char *scratch, size_t bytes, cudaStream_t s);

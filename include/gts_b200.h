@@ -132,6 +132,19 @@ int gts_filter_timing(gts_index *idx, int reset, double *ms, long long *launches
  * launched for searches on this handle (a host-side count, cumulative). */
 int gts_kernel_launches(const gts_index *idx, long long *count);
 
+/* No counterpart in the reference (its launch shapes are compile-time
+ * constants, search_v2.cuh: THREAD_NUM).  The GTS_FORM_FAST configuration
+ * used for k on this index.  The first batch of at least 2048 queries with a
+ * given k is run once per candidate -- learned-radius seed on or off (when a
+ * model is trained), 4 / 2 / 1 epilogue warps per query lane, 8 / 16 / 32
+ * blocks per work item -- and the fastest is kept (every candidate returns
+ * the same exact answers).  *tuned = 0 reports the default that smaller
+ * batches use.  Any output pointer may be NULL. */
+int gts_fast_config(const gts_index *idx, int k, int *tuned, int *learned, int *col_groups, int *item_blocks);
+
+/* Forget the tuned configurations (the next large batch tunes again). */
+int gts_fast_autotune_reset(gts_index *idx);
+
 /* ---------------------------------------------------------------- search */
 
 /* searchIndexKnnV2 (search_v2.cuh:975-1228) -> res_dis.

@@ -67,3 +67,23 @@ def test_fast_batches_larger_than_one_run(oracle):
     np.testing.assert_array_equal(ids, bi)
     np.testing.assert_array_equal(kth, bk)
     np.testing.assert_array_equal(dis, bd)
+
+
+def test_autotuner_picks_a_config_and_stays_exact(oracle):
+    """The first batch of >= 2048 queries for a k times every candidate
+    configuration (all exact) and keeps the fastest; later calls use it."""
+    rows = G.gmm_rows(30000, 64, 24, 0.25, seed=21)
+    ds = oracle.Dataset(2, rows)
+    q = G.query_ids(30000, 2500, seed=22)
+    with gts.Index(rows, 2, max_h=5) as idx:
+        assert not idx.fast_config(8)["tuned"]
+        kth, ids, _ = idx.knn(q, 8, form=gts.FORM_FAST, return_ids=True)
+        cfg = idx.fast_config(8)
+        assert cfg["tuned"] and cfg["col_groups"] in (1, 2, 4) and cfg["item_blocks"] in (8, 16, 32)
+        bk, bi, _ = oracle.knn_brute(ds, q, 8)
+        np.testing.assert_array_equal(ids, bi)
+        np.testing.assert_array_equal(kth, bk)
+        kth2 = idx.knn(q[:100], 8, form=gts.FORM_FAST)   # small batch: the tuned config, no retuning
+        np.testing.assert_array_equal(kth2, bk[:100])
+        idx.fast_autotune_reset()
+        assert not idx.fast_config(8)["tuned"]
