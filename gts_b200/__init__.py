@@ -278,6 +278,17 @@ class Index:
         return {"tuned": bool(v[0].value), "learned_seed": bool(v[1].value), "col_groups": v[2].value,
                 "item_blocks": v[3].value}
 
+    def fast_graphs(self, on=None) -> int:
+        """Turn the captured filter graph on/off (None: leave it); returns the
+        number of graph replays so far."""
+        n = C.c_longlong()
+        _check(self._lib.gts_fast_graphs(self._h, -1 if on is None else int(bool(on)), C.byref(n)))
+        return n.value
+
+    def set_fast_config(self, k: int, learned_seed: bool, col_groups: int, item_blocks: int = 16):
+        """Pin the fast-form configuration for k instead of tuning it."""
+        _check(self._lib.gts_fast_config_set(self._h, k, int(bool(learned_seed)), col_groups, item_blocks))
+
     def fast_autotune_reset(self):
         _check(self._lib.gts_fast_autotune_reset(self._h))
 

@@ -379,6 +379,11 @@ extern "C" void gts_index_free(gts_index *idx)
     if (idx->d_status) cudaFree(idx->d_status);
     if (idx->d_stats) cudaFree(idx->d_stats);
     if (idx->scratch) cudaFree(idx->scratch);
+    if (idx->io) cudaFree(idx->io);
+    if (idx->graph_exec) cudaGraphExecDestroy(idx->graph_exec);
+    if (idx->graph_stream) cudaStreamDestroy(idx->graph_stream);
+    for (int i = 0; i < 2; i++)
+        if (idx->graph_ev[i]) cudaEventDestroy(idx->graph_ev[i]);
     if (idx->mlp_P) cudaFree(idx->mlp_P);
     if (idx->mlp_norm) cudaFree(idx->mlp_norm);
     if (idx->mlp_piv) cudaFree(idx->mlp_piv);
@@ -454,6 +459,26 @@ struct DevBuf {
     }
 };
 
+// Carves consecutive 256-byte aligned buffers out of idx->io.
+struct IoCarve {
+    size_t sizes[6];
+    int n = 0;
+    void add(size_t b) { sizes[n++] = (b + 255) & ~(size_t)255; }
+    int get(gts_index *idx, void **out)
+    {
+        size_t total = 0;
+        for (int i = 0; i < n; i++) total += sizes[i];
+        int rc = gts::ensure_io(idx, total);
+        if (rc) return rc;
+        unsigned char *p = (unsigned char *)idx->io;
+        for (int i = 0; i < n; i++) {
+            out[i] = p;
+            p += sizes[i];
+        }
+        return GTS_OK;
+    }
+};
+
 int check_qids(const gts_index *idx, const int *qids, int qnum)
 {
     for (int i = 0; i < qnum; i++) {
@@ -487,11 +512,14 @@ extern "C" int gts_knn(gts_index *idx, const int *qids, int qnum, int k, int for
     int rc = check_qids(idx, qids, qnum);
     if (rc) return rc;
     cudaStream_t s = idx->stream;
-    DevBuf bq, bk, bi, bd;
-    if ((rc = bq.alloc(sizeof(int) * (size_t)qnum)) || (rc = bk.alloc(sizeof(float) * (size_t)qnum)))
-        return rc;
-    if (ids_out && (rc = bi.alloc(sizeof(int) * (size_t)qnum * (k > 0 ? k : 1)))) return rc;
-    if (dists_out && (rc = bd.alloc(sizeof(float) * (size_t)qnum * (k > 0 ? k : 1)))) return rc;
+    IoCarve io;
+    io.add(sizeof(int) * (size_t)qnum);
+    io.add(sizeof(float) * (size_t)qnum);
+    io.add(ids_out ? sizeof(int) * (size_t)qnum * (k > 0 ? k : 1) : 0);
+    io.add(dists_out ? sizeof(float) * (size_t)qnum * (k > 0 ? k : 1) : 0);
+    void *buf[4];
+    if ((rc = io.get(idx, buf))) return rc;
+    struct { void *p; } bq{buf[0]}, bk{buf[1]}, bi{ids_out ? buf[2] : nullptr}, bd{dists_out ? buf[3] : nullptr};
     GTS_CUDA_TRY(cudaMemcpyAsync(bq.p, qids, sizeof(int) * (size_t)qnum, cudaMemcpyHostToDevice, s));
     rc = gts::search_knn(idx, (int *)bq.p, qnum, k, form, (float *)bk.p, (int *)bi.p, (float *)bd.p, s);
     if (rc) return rc;
@@ -524,8 +552,12 @@ extern "C" int gts_range(gts_index *idx, const int *qids, int qnum, float r, int
     int rc = check_qids(idx, qids, qnum);
     if (rc) return rc;
     cudaStream_t s = idx->stream;
-    DevBuf bq, bc;
-    if ((rc = bq.alloc(sizeof(int) * (size_t)qnum)) || (rc = bc.alloc(sizeof(int) * (size_t)qnum))) return rc;
+    IoCarve io;
+    io.add(sizeof(int) * (size_t)qnum);
+    io.add(sizeof(int) * (size_t)qnum);
+    void *buf[2];
+    if ((rc = io.get(idx, buf))) return rc;
+    struct { void *p; } bq{buf[0]}, bc{buf[1]};
     GTS_CUDA_TRY(cudaMemcpyAsync(bq.p, qids, sizeof(int) * (size_t)qnum, cudaMemcpyHostToDevice, s));
     rc = gts::search_range(idx, (int *)bq.p, qnum, r, (int *)bc.p, nullptr, s);
     if (rc) return rc;

@@ -219,6 +219,23 @@ int ensure_scratch(gts_index *idx, size_t bytes)
     return GTS_OK;
 }
 
+int ensure_io(gts_index *idx, size_t bytes)
+{
+    if (bytes <= idx->io_bytes) return GTS_OK;
+    if (idx->io) cudaFree(idx->io);
+    idx->io = nullptr;
+    idx->io_bytes = 0;
+    size_t want = bytes + bytes / 4 + 4096;
+    if (cudaMalloc(&idx->io, want) != cudaSuccess) {
+        cudaGetLastError();
+        idx->io = nullptr;
+        gts_set_error("cudaMalloc of %zu bytes of argument buffers failed", want);
+        return GTS_ERR_NOMEM;
+    }
+    idx->io_bytes = want;
+    return GTS_OK;
+}
+
 void free_tree(gts_index *idx)
 {
     if (idx->fast_recs) cudaFree(idx->fast_recs);
@@ -226,6 +243,7 @@ void free_tree(gts_index *idx)
     idx->fast_nb = 0;
     idx->fast_nsb = 0;
     for (int &c : idx->fast_cfg) c = 0;
+    graph_invalidate(idx);
     idx->mlp_ready = false;   // its feature pivots belong to the old tree
     void *ps[] = {idx->trows, idx->tstrs, idx->tlens, idx->id_list, idx->pos_of_id, idx->node_pid,
                   idx->node_size, idx->node_lid, idx->node_pivot, idx->node_min_dis,
@@ -240,6 +258,7 @@ void free_tree(gts_index *idx)
 
 void free_data(gts_index *idx)
 {
+    graph_invalidate(idx);   // the captured filter pass reads the rows
     if (idx->rows) cudaFree(idx->rows);
     if (idx->strs) cudaFree(idx->strs);
     if (idx->lens) cudaFree(idx->lens);

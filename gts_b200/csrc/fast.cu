@@ -1239,9 +1239,15 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
 // d_fail and counted in *n_fail; *r2_out (nullable) receives the run's final
 // bounds (valid until the region is reused).  region: scratch of at least
 // plan_run(qnum) bytes.
-static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, const int *d_qids, int qnum, int k,
-                    const FastCfg &cfg, bool learned, const int *carry, float *d_kth, int *d_ids, float *d_dists,
-                    int *d_fail, int *n_fail, int **r2_out, cudaStream_t st)
+// The kernels of one filter run over a query batch, enqueued on `st` with no
+// host synchronisation (so the sequence can be captured in a CUDA graph).
+// learned: also seed each query's bound from the learned radius model.
+// carry (nullable): certified starting bounds (float bits, one per query).
+// Queries the run cannot answer (a learned seed below the k-th distance, or
+// a full candidate list) are written to d_fail, their count to r.ctr[0].
+static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids, int qnum, int k, const FastCfg &cfg,
+                            bool learned, const int *carry, float *d_kth, int *d_ids, float *d_dists, int *d_fail,
+                            bool timed, bool capturing, cudaStream_t st)
 {
     const FastShape fs = fast_shape(idx->dim);
     const int ntiles = (qnum + kFT - 1) / kFT;
@@ -1249,12 +1255,6 @@ static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, 
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    RunBufs r;
-    const size_t need = plan_run(idx, qnum, region, &r);
-    if (need > region_bytes) {
-        gts_set_error("filter run needs %zu bytes of scratch, the region holds %zu", need, region_bytes);
-        return GTS_ERR_INVALID;
-    }
     int rc;
     const FastSummary bs = fast_summary(idx->fast_recs, fs, nb, nsb, idx->num);
 
@@ -1305,11 +1305,13 @@ static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, 
     a.item_counter = r.ctr + 1;
     a.status = idx->d_status;
     a.stats = idx->d_stats;
-    const bool timed = idx->time_filter && idx->fev[0];
-    if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[0], st));
+    // events inside a captured graph must be external records to time it
+    if (timed)
+        GTS_CUDA_TRY(cudaEventRecordWithFlags(idx->fev[0], st, capturing ? cudaEventRecordExternal : 0));
     if ((rc = launch_fast_tile(a, cfg.cg, nsm, st))) return rc;
     idx->kernel_launches++;
-    if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[1], st));
+    if (timed)
+        GTS_CUDA_TRY(cudaEventRecordWithFlags(idx->fev[1], st, capturing ? cudaEventRecordExternal : 0));
     k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 1ull);
     idx->kernel_launches++;
     k_fast_final<<<qnum, 128, 0, st>>>(idx->rows, idx->dim, idx->num, bs.ids, nb * kFB, d_qids, k,
@@ -1317,6 +1319,12 @@ static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, 
                                         d_dists, d_fail, r.ctr, idx->d_stats);
     idx->kernel_launches++;
     GTS_CUDA_TRY(cudaGetLastError());
+    return GTS_OK;
+}
+
+// After a run: kernel status and failure count back on the host.
+static int fast_run_finish(gts_index *idx, const RunBufs &r, int *n_fail, int **r2_out, bool timed, cudaStream_t st)
+{
     int status = 0;
     GTS_CUDA_TRY(cudaMemcpyAsync(&status, idx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
     GTS_CUDA_TRY(cudaMemcpyAsync(n_fail, r.ctr, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1333,6 +1341,25 @@ static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, 
     }
     if (r2_out) *r2_out = r.r2;
     return GTS_OK;
+}
+
+// One filter run, launched directly.  region: scratch of at least
+// plan_run(qnum) bytes.
+static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, const int *d_qids, int qnum, int k,
+                    const FastCfg &cfg, bool learned, const int *carry, float *d_kth, int *d_ids, float *d_dists,
+                    int *d_fail, int *n_fail, int **r2_out, cudaStream_t st)
+{
+    RunBufs r;
+    const size_t need = plan_run(idx, qnum, region, &r);
+    if (need > region_bytes) {
+        gts_set_error("filter run needs %zu bytes of scratch, the region holds %zu", need, region_bytes);
+        return GTS_ERR_INVALID;
+    }
+    const bool timed = idx->time_filter && idx->fev[0];
+    int rc = fast_run_enqueue(idx, r, d_qids, qnum, k, cfg, learned, carry, d_kth, d_ids, d_dists, d_fail, timed,
+                              false, st);
+    if (rc) return rc;
+    return fast_run_finish(idx, r, n_fail, r2_out, timed, st);
 }
 
 // Bookkeeping of one re-answer stage: the failed queries' positions in the
@@ -1362,6 +1389,13 @@ struct FastCall {
     size_t region_bytes;
     Book book[3];   // stage 0: unseeded filter, 1: filter from the bound reached, 2: plain traversal
 };
+
+void graph_invalidate(gts_index *idx)
+{
+    if (idx->graph_exec) cudaGraphExecDestroy(idx->graph_exec);
+    idx->graph_exec = nullptr;
+    for (long long &v : idx->graph_key) v = 0;
+}
 
 // Queries listed in book[stage].fail (indices into parent_q) answered again:
 // 0 -> after a learned run: the filter without the learned seed;
@@ -1405,6 +1439,82 @@ static int rerun_failed(gts_index *idx, FastCall &fc, const FastCfg &cfg, int st
     return GTS_OK;
 }
 
+// One batch (at most one filter run) through the CUDA graph of the filter
+// pass: the pass (sort, seeds, pruning, filter, recheck: 11-12 kernels and
+// the CUB sort) is captured once per batch shape and argument buffers and
+// replayed on the handle's own stream.  The host then reads the failure
+// count and runs any re-answer stage directly.  Returns 1 (nothing done)
+// when the caller's buffers moved since the last capture as well: such
+// callers are better served by direct launches.  The caller has reset
+// status and counters on st.
+static int fast_search_graph(gts_index *idx, FastCall &fc, const FastCfg &cfg, const int *d_qids, int qnum, int k,
+                             float *d_kth, int *d_ids, float *d_dists, cudaStream_t st)
+{
+    if (!idx->graph_stream) {
+        GTS_CUDA_TRY(cudaStreamCreateWithFlags(&idx->graph_stream, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; i++) GTS_CUDA_TRY(cudaEventCreateWithFlags(&idx->graph_ev[i], cudaEventDisableTiming));
+    }
+    cudaStream_t gs = idx->graph_stream;
+    const bool learned = cfg.learned && idx->mlp_ready;
+    const bool timed = idx->time_filter && idx->fev[0];
+    const int first = learned ? 0 : 1;
+    RunBufs r;
+    plan_run(idx, qnum, fc.region, &r);
+    const long long key[8] = {qnum, k,
+                              cfg_pack(cfg) | (learned ? 1 << 16 : 0) | (timed ? 1 << 19 : 0),
+                              (long long)(uintptr_t)fc.region, (long long)(uintptr_t)idx->fast_recs,
+                              (long long)(uintptr_t)d_qids, (long long)(uintptr_t)d_kth,
+                              (long long)(uintptr_t)d_ids ^ ((long long)(uintptr_t)d_dists << 1)};
+    bool same = idx->graph_exec != nullptr;
+    for (int i = 0; i < 8 && same; i++) same = idx->graph_key[i] == key[i];
+    if (!same) {
+        // the same shape with other buffers twice in a row: launch directly
+        bool shape_same = idx->graph_exec != nullptr;
+        for (int i = 0; i < 5 && shape_same; i++) shape_same = idx->graph_key[i] == key[i];
+        if (shape_same && idx->graph_moved) return 1;
+        idx->graph_moved = shape_same;
+        graph_invalidate(idx);
+        const long long l0 = idx->kernel_launches;
+        GTS_CUDA_TRY(cudaStreamBeginCapture(gs, cudaStreamCaptureModeRelaxed));
+        int rc = fast_run_enqueue(idx, r, d_qids, qnum, k, cfg, learned, nullptr, d_kth, d_ids, d_dists,
+                                  fc.book[first].fail, timed, true, gs);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(gs, &g);
+        idx->kernel_launches = l0;   // counted at every replay instead
+        if (rc || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            if (!rc) gts_set_error("filter graph capture failed: %s", cudaGetErrorString(e));
+            cudaGetLastError();
+            return rc ? rc : GTS_ERR_CUDA;
+        }
+        e = cudaGraphInstantiate(&idx->graph_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            idx->graph_exec = nullptr;
+            gts_set_error("filter graph instantiation failed: %s", cudaGetErrorString(e));
+            return GTS_ERR_CUDA;
+        }
+        for (int i = 0; i < 8; i++) idx->graph_key[i] = key[i];
+        // this library's kernels in the graph (CUB's and memsets not counted)
+        idx->graph_kernels = learned ? 12 : 11;
+    } else {
+        idx->graph_moved = false;
+    }
+    GTS_CUDA_TRY(cudaEventRecord(idx->graph_ev[0], st));
+    GTS_CUDA_TRY(cudaStreamWaitEvent(gs, idx->graph_ev[0], 0));
+    GTS_CUDA_TRY(cudaGraphLaunch(idx->graph_exec, gs));
+    idx->kernel_launches += idx->graph_kernels;
+    idx->graph_launches++;
+    int n_fail = 0, *r2 = nullptr, rc;
+    if ((rc = fast_run_finish(idx, r, &n_fail, &r2, timed, gs))) return rc;
+    if (n_fail > 0 && (rc = rerun_failed(idx, fc, cfg, first, d_qids, n_fail, r2, k, d_kth, d_ids, d_dists, gs)))
+        return rc;
+    idx->last_fast_overflow = n_fail;
+    GTS_CUDA_TRY(cudaEventRecord(idx->graph_ev[1], gs));
+    GTS_CUDA_TRY(cudaStreamWaitEvent(st, idx->graph_ev[1], 0));
+    return GTS_OK;
+}
+
 // The whole batch with one configuration: filter runs of at most qc
 // queries, each followed by the re-answer stages its failures need.
 static int fast_search_cfg(gts_index *idx, FastCall &fc, int qc, const FastCfg &cfg, const int *d_qids, int qnum,
@@ -1415,6 +1525,14 @@ static int fast_search_cfg(gts_index *idx, FastCall &fc, int qc, const FastCfg &
     const bool learned = cfg.learned && idx->mlp_ready;
     const int first = learned ? 0 : 1;
     int total_fail = 0, rc;
+    if (idx->use_graphs && qnum <= qc) {
+        rc = fast_search_graph(idx, fc, cfg, d_qids, qnum, k, d_kth, d_ids, d_dists, st);
+        if (rc < 0) return rc;
+        if (rc == 0) {
+            GTS_CUDA_TRY(cudaStreamSynchronize(st));
+            return GTS_OK;
+        }
+    }
     for (int q0 = 0; q0 < qnum; q0 += qc) {
         const int qn = std::min(qc, qnum - q0);
         int n_fail = 0, *r2 = nullptr;
@@ -1581,6 +1699,32 @@ extern "C" int gts_fast_config(const gts_index *idx, int k, int *tuned, int *lea
         return GTS_ERR_INVALID;
     }
     return gts::fast_config_get(idx, k, tuned, learned, col_groups, item_blocks);
+}
+
+extern "C" int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int item_blocks)
+{
+    if (!idx || k < 1 || k > gts::kFMaxK || (col_groups != 1 && col_groups != 2 && col_groups != 4) ||
+        col_groups * k > 64 || (item_blocks != 8 && item_blocks != 16 && item_blocks != 32)) {
+        gts_set_error("gts_fast_config_set: k in [1, 64], column groups 1/2/4 with groups * k <= 64, "
+                      "8/16/32 blocks per item");
+        return GTS_ERR_INVALID;
+    }
+    idx->fast_cfg[k] = gts::cfg_pack(gts::FastCfg{learned != 0, col_groups, item_blocks});
+    return GTS_OK;
+}
+
+extern "C" int gts_fast_graphs(gts_index *idx, int on, long long *replays)
+{
+    if (!idx) {
+        gts_set_error("null index");
+        return GTS_ERR_INVALID;
+    }
+    if (on >= 0) {
+        idx->use_graphs = on != 0;
+        if (!idx->use_graphs) gts::graph_invalidate(idx);
+    }
+    if (replays) *replays = idx->graph_launches;
+    return GTS_OK;
 }
 
 extern "C" int gts_fast_autotune_reset(gts_index *idx)

@@ -45,6 +45,20 @@ struct gts_index {
     // reusable per-call scratch (grown on demand, freed with the handle)
     void *scratch = nullptr;
     size_t scratch_bytes = 0;
+    // device copies of host-buffer arguments (gts_knn, gts_range, ...):
+    // grown on demand and kept, so those calls allocate nothing in steady state
+    void *io = nullptr;
+    size_t io_bytes = 0;
+    // CUDA graph of the fast form's filter pass (fast.cu), launched on the
+    // handle's own stream and replayed while the batch shape stays the same
+    cudaStream_t graph_stream = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    long long graph_key[8] = {};
+    cudaEvent_t graph_ev[2] = {nullptr, nullptr};
+    bool use_graphs = true;
+    long long graph_launches = 0;
+    long long graph_kernels = 0;   // this library's kernels in the captured graph
+    bool graph_moved = false;      // the last capture was for moved argument buffers
 
     // learned kNN radius (mlp.cu): parameters, input standardisation,
     // feature pivots; valid for the tree it was trained on
@@ -86,12 +100,16 @@ int dev_alloc(T **p, size_t n, size_t *acct);
 
 // Grow idx->scratch to at least `bytes`.
 int ensure_scratch(gts_index *idx, size_t bytes);
+// Grow idx->io to at least `bytes`.
+int ensure_io(gts_index *idx, size_t bytes);
 
 bool fast_supported(const gts_index *idx, int k);
 int mlp_seed(gts_index *idx, const int *d_qids, int qnum, int k, int *d_r2_bits, cudaStream_t st);
 int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                     float *d_dists, cudaStream_t s);
 int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *cg, int *item);
+// Drop the captured filter graph (its device pointers or parameters changed).
+void graph_invalidate(gts_index *idx);
 // Unseeded filter with all scratch inside the caller's fixed buffer.
 int search_knn_fast_fixed(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                           float *d_dists, unsigned char *scratch, size_t bytes, cudaStream_t s);

@@ -486,6 +486,7 @@ int mlp_train(gts_index *idx, int n_train, int k_max, int epochs, unsigned seed,
     idx->mlp_widen = std::exp(std::max(q, 0.f)) * 1.001f;
     idx->mlp_ready = true;
     for (int &c : idx->fast_cfg) c = 0;   // tuned with the previous seeds
+    graph_invalidate(idx);                 // captured the previous model's scalars
     if (val_rmse) *val_rmse = (float)std::sqrt(se / n_val);
     if (widen_out) *widen_out = idx->mlp_widen;
     return GTS_OK;

@@ -142,8 +142,22 @@ int gts_kernel_launches(const gts_index *idx, long long *count);
  * batches use.  Any output pointer may be NULL. */
 int gts_fast_config(const gts_index *idx, int k, int *tuned, int *learned, int *col_groups, int *item_blocks);
 
+/* Pin the configuration for k (learned seed 0/1, 1/2/4 column groups with
+ * groups * k <= 64, 8/16/32 blocks per item) instead of tuning it. */
+int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int item_blocks);
+
 /* Forget the tuned configurations (the next large batch tunes again). */
 int gts_fast_autotune_reset(gts_index *idx);
+
+/* No counterpart in the reference (it launches and synchronises every kernel
+ * from the host, search_v2.cuh:868-871).  A GTS_FORM_FAST batch of at most
+ * 32,768 queries runs its filter pass as a CUDA graph, captured once per
+ * batch shape and argument buffers and replayed on the handle's own stream
+ * (ordered after and before the caller's stream by events); a caller whose
+ * buffers move from call to call gets direct launches instead.  on = 1 / 0 turns this on (the
+ * default) / off, on < 0 leaves it; *replays (nullable) receives the number
+ * of graph launches so far. */
+int gts_fast_graphs(gts_index *idx, int on, long long *replays);
 
 /* ---------------------------------------------------------------- search */
 

@@ -87,3 +87,25 @@ def test_autotuner_picks_a_config_and_stays_exact(oracle):
         np.testing.assert_array_equal(kth2, bk[:100])
         idx.fast_autotune_reset()
         assert not idx.fast_config(8)["tuned"]
+
+
+def test_graph_replay_equals_direct_launches(oracle):
+    """The filter pass captured in a CUDA graph and replayed gives the same
+    answers as the directly launched kernels, across repeated calls and a
+    change of batch shape (which captures again)."""
+    rows = G.gmm_rows(25000, 128, 20, 0.2, seed=51)
+    ds = oracle.Dataset(2, rows)
+    q1 = G.query_ids(25000, 700, seed=52)
+    q2 = G.query_ids(25000, 333, seed=53)
+    with gts.Index(rows, 2, max_h=5) as idx:
+        idx.fast_graphs(False)
+        direct = [idx.knn(q, 8, form=gts.FORM_FAST, return_ids=True) for q in (q1, q2)]
+        idx.fast_graphs(True)
+        n0 = idx.fast_graphs()
+        for q, want in ((q1, direct[0]), (q1, direct[0]), (q2, direct[1]), (q2, direct[1]), (q1, direct[0])):
+            got = idx.knn(q, 8, form=gts.FORM_FAST, return_ids=True)   # captured, replayed, captured, ...
+            for x, y in zip(got, want):
+                np.testing.assert_array_equal(x, y)
+        assert idx.fast_graphs() - n0 == 5
+    bk, bi, _ = oracle.knn_brute(ds, q1, 8)
+    np.testing.assert_array_equal(direct[0][1], bi)

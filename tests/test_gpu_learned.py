@@ -67,6 +67,9 @@ def test_learned_radius_gain(learned_index):
     q = G.query_ids(len(rows), 2000, seed=43)
     with gts.Index(rows, 2, max_h=5) as plain:
         for k in (8, 32, 64):
+            cg = 4 if k <= 16 else (2 if k <= 32 else 1)
+            idx.set_fast_config(k, True, cg)      # the learned seed on, whatever the tuner would pick
+            plain.set_fast_config(k, False, cg)
             idx.knn(q, k, form=gts.FORM_FAST)
             learned = idx.search_stats()
             plain.knn(q, k, form=gts.FORM_FAST)
