@@ -29,12 +29,12 @@ import numpy as np
 
 __all__ = ["GtsError", "Params", "Index", "load", "load_queries", "load_updates",
            "indexConstru", "searchIndexKnnV2", "searchIndexRnnV2", "updateIndexRnn",
-           "saveK", "saveR", "lib_path", "FORM_PLAIN", "FORM_FAST"]
+           "saveK", "saveR", "lib_path", "FORM_PLAIN", "FORM_FAST", "FORM_PLAIN_LEARNED"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libgts_b200.so")
 STR_STRIDE = 109
-FORM_PLAIN, FORM_FAST = 0, 1
+FORM_PLAIN, FORM_FAST, FORM_PLAIN_LEARNED = 0, 1, 2
 RADIUS_MODEL_PARAMS = 128 * 33 + 128 + 128 * 128 + 128 + 128 + 1
 _lib = None
 

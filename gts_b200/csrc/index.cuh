@@ -107,6 +107,8 @@ bool fast_supported(const gts_index *idx, int k);
 int mlp_seed(gts_index *idx, const int *d_qids, int qnum, int k, int *d_r2_bits, cudaStream_t st);
 int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                     float *d_dists, cudaStream_t s);
+int search_knn_plain_learned(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
+                             float *d_dists, cudaStream_t s);
 int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *cg, int *item);
 // Drop the captured filter graph (its device pointers or parameters changed).
 void graph_invalidate(gts_index *idx);

@@ -36,7 +36,8 @@ namespace gts {
 
 constexpr int kThreads = 128;
 constexpr int kWarps = kThreads / 32;
-constexpr int kBatch = 32;
+constexpr int kBatch = 32;            // stack entries popped per step (one warp lane each)
+constexpr int kRows = 8;              // leaf rows per warp in flight
 constexpr int kStackCap = 2048;
 constexpr int kLeafObjCap = 1024;     // objects verified per step
 constexpr int kMaxK = 256;
@@ -63,6 +64,11 @@ struct SearchArgs {
     const uint32_t *deleted;
     int *counter;
     int *status;
+    // kNN seeded by the learned radius (nullable): squared radius per query
+    // (float bits); a query with fewer than k objects inside is listed in
+    // fail / n_fail instead of answered
+    const int *seed_r2_bits;
+    int *fail, *n_fail;
     unsigned long long *stats;   // [objects filtered, pivots evaluated, exact values, queries]
     float rel_eps;   // relative pruning slack
     float abs_eps;   // absolute pruning slack
@@ -164,20 +170,23 @@ __device__ __forceinline__ float warp_row_value(const float *__restrict__ row,
     return metric == kLinf ? warp_max(acc) : warp_sum(acc);
 }
 
-// Four rows at once (independent loads in flight): out[u] as warp_row_value.
-__device__ __forceinline__ void warp_row_value4(const float *const (&rows)[4], const float *__restrict__ q,
-                                                int dim, int metric, int lane, float (&out)[4])
+// R rows at once (independent loads in flight): out[u] as warp_row_value.
+template <int R>
+__device__ __forceinline__ void warp_row_values(const float *const (&rows)[R], const float *__restrict__ q,
+                                                int dim, int metric, int lane, float (&out)[R])
 {
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    float acc[R];
+#pragma unroll
+    for (int u = 0; u < R; u++) acc[u] = 0.f;
     if ((dim & 3) == 0) {
         const float4 *q4 = reinterpret_cast<const float4 *>(q);
         for (int j = lane; j < (dim >> 2); j += 32) {
-            float4 x[4];
+            float4 x[R];
 #pragma unroll
-            for (int u = 0; u < 4; u++) x[u] = __ldg(reinterpret_cast<const float4 *>(rows[u]) + j);
+            for (int u = 0; u < R; u++) x[u] = __ldg(reinterpret_cast<const float4 *>(rows[u]) + j);
             const float4 y = q4[j];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < R; u++) {
                 float d0 = x[u].x - y.x, d1 = x[u].y - y.y, d2 = x[u].z - y.z, d3 = x[u].w - y.w;
                 if (metric == kL2) {
                     acc[u] = fmaf(d0, d0, acc[u]); acc[u] = fmaf(d1, d1, acc[u]);
@@ -191,12 +200,12 @@ __device__ __forceinline__ void warp_row_value4(const float *const (&rows)[4], c
         }
     } else {
         for (int j = lane; j < dim; j += 32) {
-            float x[4];
+            float x[R];
 #pragma unroll
-            for (int u = 0; u < 4; u++) x[u] = __ldg(rows[u] + j);
+            for (int u = 0; u < R; u++) x[u] = __ldg(rows[u] + j);
             const float y = q[j];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < R; u++) {
                 float d0 = x[u] - y;
                 if (metric == kL2) acc[u] = fmaf(d0, d0, acc[u]);
                 else if (metric == kL1) acc[u] += fabsf(d0);
@@ -205,7 +214,7 @@ __device__ __forceinline__ void warp_row_value4(const float *const (&rows)[4], c
         }
     }
 #pragma unroll
-    for (int u = 0; u < 4; u++) out[u] = metric == kLinf ? warp_max(acc[u]) : warp_sum(acc[u]);
+    for (int u = 0; u < R; u++) out[u] = metric == kLinf ? warp_max(acc[u]) : warp_sum(acc[u]);
 }
 
 // Interval [lo, hi] that contains both exact leaf values (F32 and F64
@@ -224,6 +233,38 @@ __device__ __forceinline__ void value_bounds(int metric, int dim, float v, doubl
     } else {
         lo = vl;
         hi = vh;
+    }
+}
+
+// Index of the leaf holding step object o: the last li < nleaf with
+// leaf_pre[li] <= o (leaf_pre ascending, at most kBatch + 1 entries).
+__device__ __forceinline__ int leaf_of(const int *leaf_pre, int nleaf, int o)
+{
+    int lo = 0, hi = nleaf - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (leaf_pre[mid] <= o) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// value_bounds in FP32: the products and square roots add at most a few
+// ulps, covered by the extra 4e-7 / 2e-7 relative margins.
+__device__ __forceinline__ void value_bounds_f(int metric, int dim, float v, float &lo, float &hi)
+{
+    if (metric == kLinf) {   // max of exactly rounded |diff|: exact
+        lo = hi = v;
+        return;
+    }
+    const float g = 2.f * f32_sum_rel_bound(dim + 32) + 4.f * 5.9604645e-8f;
+    const float vl = v * (1.f - g), vh = v * (1.f + g);
+    if (metric == kL2) {
+        lo = sqrtf(fmaxf(vl, 0.f)) * (1.f - 4e-7f);
+        hi = sqrtf(vh) * (1.f + 4e-7f);
+    } else {
+        lo = vl * (1.f - 2e-7f);
+        hi = vh * (1.f + 2e-7f);
     }
 }
 
@@ -300,7 +341,8 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
             s.cnt = 0;
             s.overflow = 0;
             s.n_obj = s.n_piv = s.n_exact = 0;
-            s.R = knn ? DBL_MAX : (double)a.r;
+            s.R = !knn ? (double)a.r
+                       : (a.seed_r2_bits ? sqrt((double)__int_as_float(a.seed_r2_bits[q])) : DBL_MAX);
         }
         if (t.metric == kEdit) {
             int m = min(max(t.lens[qid], 0), kStrStride - 1);
@@ -322,42 +364,71 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
 
         // ---- traversal
         for (;;) {
-            if (tid == 0) {
-                // pop up to kBatch entries whose bound still admits results,
-                // stopping early when the leaves would exceed kLeafObjCap
-                int nint = 0, nleaf = 0, nobj = 0;
-                double R = s.R;
-                while (s.top > 0 && nint + nleaf < kBatch) {
-                    int node = s.stack_node[s.top - 1];
-                    float lb = s.stack_lb[s.top - 1];
-                    double slack = a.abs_eps + a.rel_eps * ((double)lb + (R < 1e300 ? R : 0.0));
-                    if ((double)lb > R + slack) { s.top--; continue; }
-                    if (t.node_pivot[node] >= 0) {
-                        s.bint[nint++] = node;
-                        s.top--;
-                    } else {
-                        int off = s.stack_off[s.top - 1];
-                        int sz = t.node_size[node] - off;
-                        int room = kLeafObjCap - nobj;
-                        if (room <= 0) break;
-                        int take = sz < room ? sz : room;
-                        s.leaf_pre[nleaf] = nobj;
-                        s.bleaf_off[nleaf] = off;
-                        s.bleaf[nleaf++] = node;
-                        nobj += take;
-                        if (take < sz) {   // the rest of a large leaf stays on the stack
-                            s.stack_off[s.top - 1] = off + take;
-                            break;
-                        }
-                        s.top--;
-                    }
+            if (warp == 0) {
+                // pop, in parallel, the top kBatch (= 32) entries: lane i looks
+                // at entry top-1-i.  Entries whose bound no longer admits
+                // results are dropped; internal nodes are taken; leaves are
+                // taken in stack order while their objects fit in
+                // kLeafObjCap (the first leaf that does not fit is taken in
+                // part and stays on the stack with its offset advanced, and
+                // nothing below it is popped this step).
+                const double R = s.R;
+                const int top = s.top;
+                const int n = top < kBatch ? top : kBatch;
+                const int e = top - 1 - lane;
+                const bool valid = lane < n;
+                int node = 0, off = 0, piv = -1, sz = 0;
+                bool alive = false;
+                if (valid) {
+                    node = s.stack_node[e];
+                    off = s.stack_off[e];
+                    const float lb = s.stack_lb[e];
+                    const double slack = a.abs_eps + a.rel_eps * ((double)lb + (R < 1e300 ? R : 0.0));
+                    alive = !((double)lb > R + slack);
                 }
-                s.leaf_pre[nleaf] = nobj;
-                s.nint = nint;
-                s.nleaf = nleaf;
-                s.ncpos = 0;
-                s.n_obj += nobj;
-                s.n_piv += nint;
+                if (alive) {
+                    piv = t.node_pivot[node];
+                    if (piv < 0) sz = t.node_size[node] - off;
+                }
+                const bool leaf = alive && piv < 0;
+                int incl = sz;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                const int excl = incl - sz;
+                const unsigned over = __ballot_sync(0xffffffffu, leaf && incl > kLeafObjCap);
+                const int stop = over ? __ffs(over) - 1 : n;   // first leaf that does not fit
+                const bool take_int = alive && !leaf && lane < stop;
+                const bool take_leaf = leaf && (lane < stop || (lane == stop && excl < kLeafObjCap));
+                const unsigned mi = __ballot_sync(0xffffffffu, take_int);
+                const unsigned ml = __ballot_sync(0xffffffffu, take_leaf);
+                const unsigned below = (1u << lane) - 1u;
+                if (take_int) s.bint[__popc(mi & below)] = node;
+                if (take_leaf) {
+                    const int li = __popc(ml & below);
+                    s.bleaf[li] = node;
+                    s.bleaf_off[li] = off;
+                    s.leaf_pre[li] = excl;
+                    if (lane == stop) s.stack_off[e] = off + (kLeafObjCap - excl);   // the rest stays
+                }
+                const int nint = __popc(mi), nleaf = __popc(ml);
+                int nobj = 0;
+                if (nleaf > 0) {
+                    const int last = 31 - __clz(ml);   // the last taken leaf lane
+                    const int lincl = __shfl_sync(0xffffffffu, incl, last);
+                    nobj = lincl < kLeafObjCap ? lincl : kLeafObjCap;
+                }
+                if (lane == 0) {
+                    s.top = top - stop;
+                    s.leaf_pre[nleaf] = nobj;
+                    s.nint = nint;
+                    s.nleaf = nleaf;
+                    s.ncpos = 0;
+                    s.n_obj += nobj;
+                    s.n_piv += nint;
+                }
             }
             __syncthreads();
             const int nint = s.nint, nleaf = s.nleaf;
@@ -367,45 +438,45 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
             // ---- leaves: filter every object, collect those needing exact values
             if (nleaf > 0) {
                 if (warp_filter) {
-                    // four rows per warp step: their loads are in flight together
-                    for (int o0 = warp * 4; o0 < nobj; o0 += kWarps * 4) {
-                        int pos[4], id[4];
-                        const float *rp[4];
-#pragma unroll
-                        for (int u = 0; u < 4; u++) {
-                            int o = min(o0 + u, nobj - 1);
-                            int li = 0;
-                            while (s.leaf_pre[li + 1] <= o) li++;
-                            pos[u] = t.node_lid[s.bleaf[li]] + s.bleaf_off[li] + (o - s.leaf_pre[li]);
-                            id[u] = t.id_list[pos[u]];
-                            rp[u] = t.trows + (size_t)pos[u] * t.dim;
+                    // kRows rows per warp step: their loads are in flight
+                    // together.  Lane u < kRows finds row u's leaf (binary
+                    // search of the step's leaf prefix) and, after the
+                    // warp-split distances, tests row u; rows run in parallel.
+                    const int nl = s.nleaf;
+                    for (int o0 = warp * kRows; o0 < nobj; o0 += kWarps * kRows) {
+                        int my_pos = 0, my_id = -1;
+                        if (lane < kRows) {
+                            const int o = min(o0 + lane, nobj - 1);
+                            const int li = leaf_of(s.leaf_pre, nl, o);
+                            my_pos = t.node_lid[s.bleaf[li]] + s.bleaf_off[li] + (o - s.leaf_pre[li]);
+                            my_id = t.id_list[my_pos];
                         }
-                        float v4[4];
-                        warp_row_value4(rp, qrow, t.dim, t.metric, lane, v4);
-                        if (lane == 0) {
-                            for (int u = 0; u < 4 && o0 + u < nobj; u++) {
-                                if (is_deleted(a.deleted, id[u])) continue;
-                                double lo, hi;
-                                value_bounds(t.metric, t.dim, v4[u], lo, hi);
-                                if (id[u] == qid) lo = hi = 0.0;
-                                if (knn) {
-                                    if (lo <= s.R) {
-                                        int c = atomicAdd(&s.ncpos, 1);
-                                        s.cpos[c] = pos[u];
-                                    }
-                                } else if (a.mode == kModeRangeCount && hi < (double)a.r * (1.0 - 2.4e-7)) {
-                                    atomicAdd(&s.cnt, 1);
-                                } else if (lo <= (double)a.r * (1.0 + 2.4e-7)) {
-                                    int c = atomicAdd(&s.ncpos, 1);
-                                    s.cpos[c] = pos[u];
-                                }
+                        const float *rp[kRows];
+#pragma unroll
+                        for (int u = 0; u < kRows; u++)
+                            rp[u] = t.trows + (size_t)__shfl_sync(0xffffffffu, my_pos, u) * t.dim;
+                        float v4[kRows];
+                        warp_row_values<kRows>(rp, qrow, t.dim, t.metric, lane, v4);
+                        float v = 0.f;
+#pragma unroll
+                        for (int u = 0; u < kRows; u++)
+                            if (lane == u) v = v4[u];
+                        if (lane < kRows && o0 + lane < nobj && !is_deleted(a.deleted, my_id)) {
+                            float lo, hi;
+                            value_bounds_f(t.metric, t.dim, v, lo, hi);
+                            if (my_id == qid) lo = hi = 0.f;
+                            if (knn) {
+                                if ((double)lo <= s.R) s.cpos[atomicAdd(&s.ncpos, 1)] = my_pos;
+                            } else if (a.mode == kModeRangeCount && (double)hi < (double)a.r * (1.0 - 2.4e-7)) {
+                                atomicAdd(&s.cnt, 1);
+                            } else if ((double)lo <= (double)a.r * (1.0 + 2.4e-7)) {
+                                s.cpos[atomicAdd(&s.ncpos, 1)] = my_pos;
                             }
                         }
                     }
                 } else {
                     for (int o = tid; o < nobj; o += kThreads) {
-                        int li = 0;
-                        while (s.leaf_pre[li + 1] <= o) li++;
+                        const int li = leaf_of(s.leaf_pre, s.nleaf, o);
                         int pos = t.node_lid[s.bleaf[li]] + s.bleaf_off[li] + (o - s.leaf_pre[li]);
                         if (is_deleted(a.deleted, t.id_list[pos])) continue;
                         int c = atomicAdd(&s.ncpos, 1);
@@ -494,13 +565,17 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
         // ---- outputs
         if (knn) {
             compact_candidates(s, a.k);
-            const int k = a.k;
+            int k = a.k;
+            if (a.seed_r2_bits && s.ncand < k) {   // the learned radius held fewer than k objects
+                if (tid == 0) a.fail[atomicAdd(a.n_fail, 1)] = q;
+                k = 0;
+            }
             for (int j = tid; j < k; j += kThreads) {
                 bool have = j < s.ncand;
                 if (a.ids) a.ids[(size_t)q * k + j] = have ? s.cid[j] : -1;
                 if (a.dists) a.dists[(size_t)q * k + j] = have ? (float)s.cd[j] : (float)t.infi_dis;
             }
-            if (tid == 0) a.kth[q] = s.ncand >= k ? (float)s.cd[k - 1] : (float)t.infi_dis;
+            if (tid == 0 && k > 0) a.kth[q] = s.ncand >= k ? (float)s.cd[k - 1] : (float)t.infi_dis;
         } else if (tid == 0) {
             if (a.mode == kModeRangeCount) a.counts[q] = s.cnt;
         }
@@ -566,6 +641,83 @@ static int run_search(gts_index *idx, SearchArgs &a, cudaStream_t st)
     return GTS_OK;
 }
 
+__global__ void k_gather_q(const int *src, const int *idx, int n, int *dst)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[idx[i]];
+}
+
+__global__ void k_scatter_q(const int *idx, int n, int k, const float *kth_s, const int *ids_s, const float *dis_s,
+                            float *kth, int *ids, float *dists)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int q = idx[i];
+    kth[q] = kth_s[i];
+    for (int j = 0; j < k; j++) {
+        if (ids) ids[(size_t)q * k + j] = ids_s[(size_t)i * k + j];
+        if (dists) dists[(size_t)q * k + j] = dis_s[(size_t)i * k + j];
+    }
+}
+
+// The plain traversal seeded by the learned radius (GTS_FORM_PLAIN_LEARNED):
+// every query starts pruning from its predicted k-th distance instead of
+// from infinity; queries whose radius held fewer than k objects are answered
+// again by the unseeded traversal, so the results are the plain form's.
+int search_knn_plain_learned(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
+                             float *d_dists, cudaStream_t st)
+{
+    size_t off = 0;
+    auto take = [&](size_t b) { size_t o = off; off += (b + 255) & ~(size_t)255; return o; };
+    const size_t o_seed = take(4 * (size_t)qnum), o_fail = take(4 * (size_t)qnum), o_n = take(16);
+    const size_t o_q = take(4 * (size_t)qnum), o_kth = take(4 * (size_t)qnum);
+    const size_t o_ids = take(4 * (size_t)qnum * k), o_dis = take(4 * (size_t)qnum * k);
+    int rc;
+    if ((rc = ensure_scratch(idx, off))) return rc;
+    unsigned char *S = (unsigned char *)idx->scratch;
+    int *seed = (int *)(S + o_seed), *fail = (int *)(S + o_fail), *n_fail = (int *)(S + o_n);
+    int *sub_q = (int *)(S + o_q), *sub_ids = d_ids ? (int *)(S + o_ids) : nullptr;
+    float *sub_kth = (float *)(S + o_kth), *sub_dis = d_dists ? (float *)(S + o_dis) : nullptr;
+    if ((rc = mlp_seed(idx, d_qids, qnum, k, seed, st))) return rc;
+    GTS_CUDA_TRY(cudaMemsetAsync(n_fail, 0, sizeof(int), st));
+    SearchArgs a{};
+    a.qids = d_qids;
+    a.qnum = qnum;
+    a.mode = kModeKnn;
+    a.k = k;
+    a.kth = d_kth;
+    a.ids = d_ids;
+    a.dists = d_dists;
+    a.seed_r2_bits = seed;
+    a.fail = fail;
+    a.n_fail = n_fail;
+    if ((rc = run_search(idx, a, st))) return rc;
+    int nf = 0;
+    GTS_CUDA_TRY(cudaMemcpyAsync(&nf, n_fail, sizeof(int), cudaMemcpyDeviceToHost, st));
+    GTS_CUDA_TRY(cudaStreamSynchronize(st));
+    idx->last_fast_overflow = nf;
+    if (nf == 0) return GTS_OK;
+    k_gather_q<<<(nf + 255) / 256, 256, 0, st>>>(d_qids, fail, nf, sub_q);
+    idx->kernel_launches++;
+    SearchArgs b{};
+    b.qids = sub_q;
+    b.qnum = nf;
+    b.mode = kModeKnn;
+    b.k = k;
+    b.kth = sub_kth;
+    b.ids = sub_ids;
+    b.dists = sub_dis;
+    idx->keep_stats = true;
+    rc = run_search(idx, b, st);
+    idx->keep_stats = false;
+    if (rc) return rc;
+    k_scatter_q<<<(nf + 255) / 256, 256, 0, st>>>(fail, nf, k, sub_kth, sub_ids, sub_dis, d_kth, d_ids, d_dists);
+    idx->kernel_launches++;
+    GTS_CUDA_TRY(cudaGetLastError());
+    GTS_CUDA_TRY(cudaStreamSynchronize(st));
+    return GTS_OK;
+}
+
 int search_knn(gts_index *idx, const int *d_qids, int qnum, int k, int form, float *d_kth, int *d_ids,
                float *d_dists, cudaStream_t st)
 {
@@ -575,6 +727,8 @@ int search_knn(gts_index *idx, const int *d_qids, int qnum, int k, int form, flo
     }
     if (form == 1 && qnum > 0 && fast_supported(idx, k))
         return search_knn_fast(idx, d_qids, qnum, k, d_kth, d_ids, d_dists, st);
+    if (form == 2 && qnum > 0 && idx->mlp_ready && idx->metric == kL2)
+        return search_knn_plain_learned(idx, d_qids, qnum, k, d_kth, d_ids, d_dists, st);
     SearchArgs a{};
     a.qids = d_qids;
     a.qnum = qnum;

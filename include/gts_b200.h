@@ -39,6 +39,8 @@ extern "C" {
 /* Search forms. */
 #define GTS_FORM_PLAIN 0     /* traversal + FP32 filter + exact recheck */
 #define GTS_FORM_FAST 1      /* learned radius + BF16 tensor-core filter + exact recheck (L2) */
+#define GTS_FORM_PLAIN_LEARNED 2  /* plain traversal seeded by the learned radius (L2, after
+                                     gts_learn_radius; otherwise the plain form) */
 
 typedef struct gts_index gts_index;
 

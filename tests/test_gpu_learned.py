@@ -77,3 +77,24 @@ def test_learned_radius_gain(learned_index):
             print(f"k={k} learned: {learned}  unlearned: {unlearned}  train: {info}")
             assert learned["appended"] < unlearned["appended"], k
             assert learned["fallback"] == 0 and unlearned["fallback"] == 0
+
+
+def test_learned_radius_seeds_the_plain_traversal(oracle, learned_index):
+    """GTS_FORM_PLAIN_LEARNED: the GTS traversal starts pruning from the
+    predicted k-th distance instead of from infinity.  Answers equal the
+    plain form's (queries whose radius held fewer than k objects are answered
+    again unseeded), and fewer leaf objects are read."""
+    rows, idx, info = learned_index
+    ds = oracle.Dataset(2, rows)
+    q = G.query_ids(len(rows), 300, seed=44)
+    for k in (1, 8, 32):
+        plain = idx.knn(q, k, form=gts.FORM_PLAIN, return_ids=True)
+        st_plain = idx.search_stats()
+        seeded = idx.knn(q, k, form=gts.FORM_PLAIN_LEARNED, return_ids=True)
+        st_seeded = idx.search_stats()
+        for x, y in zip(seeded, plain):
+            np.testing.assert_array_equal(x, y, err_msg=f"k={k}")
+        bk, bi, _ = oracle.knn_brute(ds, q, k)
+        np.testing.assert_array_equal(seeded[1], bi)
+        print(f"k={k} plain objects {st_plain['objects']} seeded objects {st_seeded['objects']}")
+        assert st_seeded["objects"] < st_plain["objects"], k
