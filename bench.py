@@ -119,7 +119,8 @@ class ClockSampler:
 def workload(args, rank=0):
     from gts_b200 import datagen as G
     rows = G.gmm_rows(args.n, args.dim, 256, 0.2, seed=args.seed)
-    qids = G.query_ids(args.n, args.queries, seed=args.seed + 1 + 7919 * rank)
+    from gts_b200 import replicas as R
+    qids = G.query_ids(args.n, args.queries, seed=R.rank_query_seed(args.seed, rank))
     return rows, qids
 
 
@@ -293,9 +294,8 @@ def run_gts(args):
     total_ms = t_start.elapsed_time(t_end)
     per_launch_ms = [a.elapsed_time(b) for a, b in ev]
     if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        from gts_b200 import replicas as R
+        total_ms = R.max_over_ranks(total_ms, dist, dev)
         dist.barrier()
     ms_per_step = total_ms / args.steps
     value = world * Q * args.steps / (total_ms / 1e3)
@@ -314,9 +314,7 @@ def run_gts(args):
         kth_e2e = idx.knn(h_q, k, form=form)
     e2e_s = time.perf_counter() - t0
     if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s = R.max_over_ranks(e2e_s, dist, dev)
     e2e = {"value": world * Q * args.steps / e2e_s, "unit": "queries/s",
            "h2d_bytes_per_step": int(h_q.nbytes), "d2h_bytes_per_step": int(kth_e2e.nbytes)}
     assert np.array_equal(kth_e2e, kth_gpu), "host-buffer and device-buffer paths disagree"
