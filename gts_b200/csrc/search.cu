@@ -34,7 +34,7 @@
 
 namespace gts {
 
-constexpr int kThreads = 128;
+constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kBatch = 32;            // stack entries popped per step (one warp lane each)
 constexpr int kRows = 8;              // leaf rows per warp in flight
