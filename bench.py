@@ -377,7 +377,8 @@ def run_gts(args):
             "dtype": "f32/f64" if args.form == "plain" else "bf16/f32/f64",
             "data": "synthetic (seeded Gaussian mixture; the paper's data sets are absent)",
             "config": config_dict(args, world), "build_s": build_s, "learned_radius": learn,
-            "autotune": idx.fast_config(k) if args.form == "fast" else None,
+            "autotune": (idx.fast_config(k) if args.form == "fast"
+                         else {"threads_per_query_cta": idx.plain_threads(0)}),
             "roofline": roofline,
             "e2e": e2e, "gpu_launches": launches, "clocks": clock_summary}
     if rank == 0 and world == 1 and args.cpu_sample > 0:

@@ -292,6 +292,17 @@ class Index:
     def fast_autotune_reset(self):
         _check(self._lib.gts_fast_autotune_reset(self._h))
 
+    def plain_threads(self, mode: int = 0) -> int:
+        """Threads per query CTA of the plain traversal for a search mode
+        (0 kNN, 1 range count, 2 range ids); 0 = not tuned yet."""
+        n = C.c_int()
+        _check(self._lib.gts_plain_threads(self._h, mode, C.byref(n)))
+        return n.value
+
+    def set_plain_threads(self, mode: int, threads: int):
+        """Pin the plain traversal's threads per query CTA (128/256/512, 0 = tune)."""
+        _check(self._lib.gts_plain_threads_set(self._h, mode, threads))
+
     def kernel_launches(self) -> int:
         """Kernels this library launched for searches on this handle so far."""
         n = C.c_longlong()

@@ -243,6 +243,7 @@ void free_tree(gts_index *idx)
     idx->fast_nb = 0;
     idx->fast_nsb = 0;
     for (int &c : idx->fast_cfg) c = 0;
+    for (int &c : idx->plain_nt) c = 0;
     graph_invalidate(idx);
     idx->mlp_ready = false;   // its feature pivots belong to the old tree
     void *ps[] = {idx->trows, idx->tstrs, idx->tlens, idx->id_list, idx->pos_of_id, idx->node_pid,

@@ -41,6 +41,9 @@ struct gts_index {
     // autotuned fast-form configuration per k (fast.cu): 0 = not tuned, else
     // 1 | learned << 1 | column groups << 2 | blocks per item << 8
     int fast_cfg[65] = {};
+    // autotuned threads per query CTA of the plain traversal per search mode
+    // (kNN, range count, range ids; search.cu), 0 = not tuned
+    int plain_nt[3] = {};
 
     // reusable per-call scratch (grown on demand, freed with the handle)
     void *scratch = nullptr;

@@ -34,8 +34,8 @@
 
 namespace gts {
 
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
+// threads per query CTA: 128, 256 or 512, picked per search mode by the
+// autotuner in run_search (warps per query)
 constexpr int kBatch = 32;            // stack entries popped per step (one warp lane each)
 constexpr int kRows = 8;              // leaf rows per warp in flight
 constexpr int kStackCap = 2048;
@@ -270,19 +270,20 @@ __device__ __forceinline__ void value_bounds_f(int metric, int dim, float v, flo
 
 // Bitonic sort of the candidate buffer by (distance, id), n entries padded
 // to the next power of two; keeps the first min(n, k).
+template <int NT>
 __device__ void compact_candidates(SearchSmem &s, int k)
 {
     int n = s.ncand;
     int p2 = 1;
     while (p2 < n) p2 <<= 1;
-    for (int i = n + threadIdx.x; i < p2; i += kThreads) {
+    for (int i = n + threadIdx.x; i < p2; i += NT) {
         s.cd[i] = DBL_MAX;
         s.cid[i] = 0x7fffffff;
     }
     __syncthreads();
     for (int size = 2; size <= p2; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int i = threadIdx.x; i < p2 / 2; i += kThreads) {
+            for (int i = threadIdx.x; i < p2 / 2; i += NT) {
                 int lo = 2 * i - (i & (stride - 1));
                 int hi = lo + stride;
                 bool up = ((lo & size) == 0);
@@ -304,7 +305,8 @@ __device__ void compact_candidates(SearchSmem &s, int k)
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
+template <int NT>
+__global__ void __launch_bounds__(NT) k_search(SearchArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SearchSmem &s = *reinterpret_cast<SearchSmem *>(smem_raw);
@@ -347,8 +349,8 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
         if (t.metric == kEdit) {
             int m = min(max(t.lens[qid], 0), kStrStride - 1);
             const char *src = t.strs + (size_t)qid * kStrStride;
-            for (int i = tid; i < kStrStride; i += kThreads) s.qstr[i] = src[i];
-            for (int c = tid; c < 256; c += kThreads) {
+            for (int i = tid; i < kStrStride; i += NT) s.qstr[i] = src[i];
+            for (int c = tid; c < 256; c += NT) {
                 uint64_t bits = 0;
                 for (int i = 0; i < m && i < 64; i++)
                     if ((unsigned char)src[i] == (unsigned)c) bits |= 1ull << i;
@@ -357,7 +359,7 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
             if (tid == 0) s.qlen = m;
         } else if (t.dim <= kMaxDimSmem) {
             const float *src = t.rows + (size_t)qid * t.dim;
-            for (int i = tid; i < t.dim; i += kThreads) s.qrow[i] = src[i];
+            for (int i = tid; i < t.dim; i += NT) s.qrow[i] = src[i];
         }
         __syncthreads();
         const float *qrow = t.dim <= kMaxDimSmem ? s.qrow : t.rows + (size_t)qid * t.dim;
@@ -443,7 +445,7 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
                     // search of the step's leaf prefix) and, after the
                     // warp-split distances, tests row u; rows run in parallel.
                     const int nl = s.nleaf;
-                    for (int o0 = warp * kRows; o0 < nobj; o0 += kWarps * kRows) {
+                    for (int o0 = warp * kRows; o0 < nobj; o0 += (NT / 32) * kRows) {
                         int my_pos = 0, my_id = -1;
                         if (lane < kRows) {
                             const int o = min(o0 + lane, nobj - 1);
@@ -475,7 +477,7 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
                         }
                     }
                 } else {
-                    for (int o = tid; o < nobj; o += kThreads) {
+                    for (int o = tid; o < nobj; o += NT) {
                         const int li = leaf_of(s.leaf_pre, s.nleaf, o);
                         int pos = t.node_lid[s.bleaf[li]] + s.bleaf_off[li] + (o - s.leaf_pre[li]);
                         if (is_deleted(a.deleted, t.id_list[pos])) continue;
@@ -487,8 +489,8 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
                 // exact values for the collected positions
                 const int ncpos = s.ncpos;
                 if (tid == 0) s.n_exact += ncpos;
-                if (knn && s.ncand + ncpos > kCandCap) compact_candidates(s, a.k);
-                for (int c = tid; c < ncpos; c += kThreads) {
+                if (knn && s.ncand + ncpos > kCandCap) compact_candidates<NT>(s, a.k);
+                for (int c = tid; c < ncpos; c += NT) {
                     int pos = s.cpos[c];
                     int id = t.id_list[pos];
                     double d = (id == qid) ? 0.0 : exact_obj(a, s, pos, acc);
@@ -507,13 +509,13 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
                     }
                 }
                 __syncthreads();
-                if (knn && s.ncand > kCandCap - kLeafObjCap) compact_candidates(s, a.k);
+                if (knn && s.ncand > kCandCap - kLeafObjCap) compact_candidates<NT>(s, a.k);
             }
 
             // ---- internal nodes: pivot distance bounds, then ring pruning of children
             if (nint > 0) {
                 if (warp_filter) {
-                    for (int b = warp; b < nint; b += kWarps) {
+                    for (int b = warp; b < nint; b += (NT / 32)) {
                         int piv = t.node_pivot[s.bint[b]];
                         float v = warp_row_value(t.rows + (size_t)piv * t.dim, qrow, t.dim, t.metric, lane);
                         if (lane == 0) {
@@ -525,7 +527,7 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
                         }
                     }
                 } else {
-                    for (int b = tid; b < nint; b += kThreads) {
+                    for (int b = tid; b < nint; b += NT) {
                         int piv = t.node_pivot[s.bint[b]];
                         double d = (piv == qid) ? 0.0 : exact_id(a, s, piv, kAccF64);
                         s.bdq_lo[b] = (float)d;
@@ -534,7 +536,7 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
                 }
                 __syncthreads();
                 const double R = s.R;
-                for (int w = tid; w < nint * O; w += kThreads) {
+                for (int w = tid; w < nint * O; w += NT) {
                     int b = w / O, i = w % O;
                     int node = s.bint[b];
                     long c = (long)node * O + i + 1;
@@ -564,13 +566,13 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
 
         // ---- outputs
         if (knn) {
-            compact_candidates(s, a.k);
+            compact_candidates<NT>(s, a.k);
             int k = a.k;
             if (a.seed_r2_bits && s.ncand < k) {   // the learned radius held fewer than k objects
                 if (tid == 0) a.fail[atomicAdd(a.n_fail, 1)] = q;
                 k = 0;
             }
-            for (int j = tid; j < k; j += kThreads) {
+            for (int j = tid; j < k; j += NT) {
                 bool have = j < s.ncand;
                 if (a.ids) a.ids[(size_t)q * k + j] = have ? s.cid[j] : -1;
                 if (a.dists) a.dists[(size_t)q * k + j] = have ? (float)s.cd[j] : (float)t.infi_dis;
@@ -593,6 +595,102 @@ __global__ void __launch_bounds__(kThreads) k_search(SearchArgs a)
 }
 
 // ---------------------------------------------------------------------------
+
+constexpr int kPlainTuneMin = 1024;
+constexpr int kPlainTuneSample = 256;
+constexpr int kPlainDefaultThreads = 256;
+
+template <int NT>
+static int launch_search_nt(gts_index *idx, const SearchArgs &a, cudaStream_t st)
+{
+    const size_t smem = sizeof(SearchSmem);
+    GTS_CUDA_TRY(cudaFuncSetAttribute(k_search<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, nsm = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search<NT>, NT, smem);
+    if (per_sm < 1) per_sm = 1;
+    int grid = nsm * per_sm;
+    if (grid > a.qnum) grid = a.qnum;
+    k_search<NT><<<grid, NT, smem, st>>>(a);
+    idx->kernel_launches++;
+    GTS_CUDA_TRY(cudaGetLastError());
+    return GTS_OK;
+}
+
+static int launch_search(gts_index *idx, const SearchArgs &a, int nt, cudaStream_t st)
+{
+    switch (nt) {
+    case 128: return launch_search_nt<128>(idx, a, st);
+    case 512: return launch_search_nt<512>(idx, a, st);
+    default: return launch_search_nt<256>(idx, a, st);
+    }
+}
+
+// Times 128 / 256 / 512 threads per query CTA on the batch's first
+// kPlainTuneSample queries (results identical; the full batch then runs with
+// the fastest).  Range-id mode is not tuned (its output offsets belong to
+// the whole batch): it takes the range-count choice.  A seeded kNN batch is
+// timed unseeded (the seeds' failure list belongs to the real run).
+static int plain_autotune(gts_index *idx, const SearchArgs &a, cudaStream_t st, int *best_nt)
+{
+    *best_nt = kPlainDefaultThreads;
+    if (a.mode == kModeRangeIds) {
+        if (idx->plain_nt[kModeRangeCount]) *best_nt = idx->plain_nt[kModeRangeCount];
+        return GTS_OK;
+    }
+    SearchArgs t = a;
+    t.qnum = kPlainTuneSample;
+    t.seed_r2_bits = nullptr;
+    cudaEvent_t e0, e1;
+    GTS_CUDA_TRY(cudaEventCreate(&e0));
+    GTS_CUDA_TRY(cudaEventCreate(&e1));
+    float best = 3.0e38f;
+    int rc = GTS_OK;
+    const int cand[3] = {128, 256, 512};
+    for (int rep = 0; rep < 2 && rc == GTS_OK; rep++)   // first pass warms caches and modules
+        for (int c : cand) {
+            cudaMemsetAsync(idx->d_counter, 0, sizeof(int), st);
+            cudaEventRecord(e0, st);
+            if ((rc = launch_search(idx, t, c, st))) break;
+            cudaEventRecord(e1, st);
+            float ms = 0.f;
+            if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+                gts_set_error("plain autotune: CUDA event failed");
+                rc = GTS_ERR_CUDA;
+                break;
+            }
+            if (rep == 1 && ms < best) {
+                best = ms;
+                *best_nt = c;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaMemsetAsync(idx->d_counter, 0, sizeof(int), st);
+    cudaMemsetAsync(idx->d_stats, 0, kStatsN * sizeof(unsigned long long), st);
+    return rc;
+}
+
+extern "C" int gts_plain_threads(const gts_index *idx, int mode, int *threads)
+{
+    if (!idx || mode < 0 || mode > 2 || !threads) {
+        gts_set_error("gts_plain_threads: null index / output or mode outside 0..2");
+        return GTS_ERR_INVALID;
+    }
+    *threads = idx->plain_nt[mode];
+    return GTS_OK;
+}
+
+extern "C" int gts_plain_threads_set(gts_index *idx, int mode, int threads)
+{
+    if (!idx || mode < 0 || mode > 2 || (threads != 0 && threads != 128 && threads != 256 && threads != 512)) {
+        gts_set_error("gts_plain_threads_set: null index, mode outside 0..2 or threads not 0/128/256/512");
+        return GTS_ERR_INVALID;
+    }
+    idx->plain_nt[mode] = threads;
+    return GTS_OK;
+}
 
 static int run_search(gts_index *idx, SearchArgs &a, cudaStream_t st)
 {
@@ -618,18 +716,18 @@ static int run_search(gts_index *idx, SearchArgs &a, cudaStream_t st)
     GTS_CUDA_TRY(cudaMemsetAsync(idx->d_counter, 0, sizeof(int), st));
     GTS_CUDA_TRY(cudaMemsetAsync(idx->d_status, 0, sizeof(int), st));
     if (!idx->keep_stats) GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, kStatsN * sizeof(unsigned long long), st));
-    size_t smem = sizeof(SearchSmem);
-    GTS_CUDA_TRY(cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int dev = 0, nsm = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search, kThreads, smem);
-    if (per_sm < 1) per_sm = 1;
-    int grid = nsm * per_sm;
-    if (grid > a.qnum) grid = a.qnum;
-    k_search<<<grid, kThreads, smem, st>>>(a);
-    idx->kernel_launches++;
-    GTS_CUDA_TRY(cudaGetLastError());
+    // threads per query CTA: tuned per search mode on the first batch of at
+    // least kPlainTuneMin queries (each candidate on the same leading
+    // kPlainTuneSample queries, CUDA events), else the tuned or default value
+    int nt = idx->plain_nt[a.mode];
+    if (!nt && a.qnum >= kPlainTuneMin && !idx->keep_stats) {
+        int rc = plain_autotune(idx, a, st, &nt);
+        if (rc) return rc;
+        idx->plain_nt[a.mode] = nt;
+    }
+    if (!nt) nt = kPlainDefaultThreads;
+    int rc = launch_search(idx, a, nt, st);
+    if (rc) return rc;
     int status = 0;
     GTS_CUDA_TRY(cudaMemcpyAsync(&status, idx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
     GTS_CUDA_TRY(cudaStreamSynchronize(st));

@@ -151,6 +151,16 @@ int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int 
 /* Forget the tuned configurations (the next large batch tunes again). */
 int gts_fast_autotune_reset(gts_index *idx);
 
+/* No counterpart in the reference (search_v2.cuh: THREAD_NUM per query
+ * block).  Threads per query CTA of the plain traversal for one search mode
+ * (0 kNN, 1 range count, 2 range ids).  The first batch of at least 1024
+ * queries of a mode times 128 / 256 / 512 on its first 256 queries and
+ * keeps the fastest (the answers do not depend on it); *threads = 0 means
+ * not tuned yet (256 is used).  _set pins it (128, 256, 512; 0 = tune
+ * again). */
+int gts_plain_threads(const gts_index *idx, int mode, int *threads);
+int gts_plain_threads_set(gts_index *idx, int mode, int threads);
+
 /* No counterpart in the reference (it launches and synchronises every kernel
  * from the host, search_v2.cuh:868-871).  A GTS_FORM_FAST batch of at most
  * 32,768 queries runs its filter pass as a CUDA graph, captured once per

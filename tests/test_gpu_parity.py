@@ -109,6 +109,37 @@ def test_range_ids(oracle):
             assert dis[offs[i] + j] == np.float32(want)
 
 
+def test_plain_thread_counts_agree_and_autotuner_picks_one(oracle):
+    """Every threads-per-query-CTA choice of the plain traversal gives the
+    same exact answers; a batch of 1024+ queries tunes the choice."""
+    rows = _data(2, 12000, 24, 17)
+    ds = oracle.Dataset(2, rows)
+    q = G.query_ids(12000, 1100, 18)
+    r = float(np.float32(G.quantile_radius(2, 0.005, 30000, 19, rows=rows)))
+    bk, bi, bd = oracle.knn_brute(ds, q[:200], 8)
+    bc = oracle.range_brute(ds, q[:200], r)
+    with gts.Index(rows, 2, max_h=4) as idx:
+        assert idx.plain_threads(0) == 0
+        kth = idx.knn(q, 8)
+        assert idx.plain_threads(0) in (128, 256, 512)
+        counts = idx.range(q, r)
+        assert idx.plain_threads(1) in (128, 256, 512)
+        for nt in (128, 256, 512):
+            for m in (0, 1, 2):
+                idx.set_plain_threads(m, nt)
+            k2, ids, dis = idx.knn(q[:200], 8, return_ids=True)
+            np.testing.assert_array_equal(k2, bk)
+            np.testing.assert_array_equal(ids, bi)
+            np.testing.assert_array_equal(dis, bd)
+            np.testing.assert_array_equal(idx.range(q[:200], r), bc)
+            c2, _, _, _ = idx.range_ids(q[:200], r)
+            np.testing.assert_array_equal(c2, bc)
+        with pytest.raises(Exception):
+            idx.set_plain_threads(0, 96)
+    np.testing.assert_array_equal(kth[:200], bk)
+    np.testing.assert_array_equal(counts[:200], bc)
+
+
 def test_update_equals_oracle(oracle):
     rows = _data(2, 1500, 10, 11)
     ds = oracle.Dataset(2, rows)
