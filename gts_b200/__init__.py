@@ -394,6 +394,45 @@ def searchIndexRnnV2(index: Index, qids, r: float) -> np.ndarray:
     return index.range(qids, r)
 
 
+def _write_fcost(fcost, values, fmt):
+    """The per-query line the reference's v1 search appends to its cost file
+    (search.cuh:857-861, 1043-1047): values separated by single spaces."""
+    if fcost is None:
+        return
+    text = "".join((fmt % v) + " " for v in values)
+    if hasattr(fcost, "write"):
+        fcost.write(text)
+        fcost.flush()
+    else:
+        with open(fcost, "a") as f:
+            f.write(text)
+
+
+def searchIndexRnn(index: Index, qids, r: float, fcost=None):
+    """searchIndexRnn, the v1 multi-query range search (search.cuh:749-889):
+    -> (qresult_count, qresult_count_prefix, result_id, result_dis), the hits
+    of query i at result_id[prefix[i] : prefix[i] + count[i]].  The same
+    traversal as the v2 entry point answers it (exact on every tree shape);
+    each query's hits come in (distance, id) order, where the reference keeps
+    its leaf-pair order (the same sets).  fcost (an open file or a path, or
+    None) receives the counts as the reference writes them."""
+    counts, offs, ids, dis = index.range_ids(qids, r)
+    _write_fcost(fcost, counts, "%d")
+    return counts, offs, ids, dis
+
+
+def searchIndexKnn(index: Index, qids, k: int, fcost=None):
+    """searchIndexKnn, the v1 multi-query kNN search (search.cuh:891-1081):
+    -> (result_id, result_dis), k entries per query at [i*k : (i+1)*k] in
+    ascending distance, ties by id (the reference breaks ties by its
+    candidate order).  Slots past the number of objects hold id -1 and
+    distance INFI_DIS.  fcost receives the k-th distances as the reference
+    writes them (%f)."""
+    kth, ids, dis = index.knn(qids, k, return_ids=True)
+    _write_fcost(fcost, kth, "%f")
+    return ids.reshape(-1), dis.reshape(-1)
+
+
 def updateIndexRnn(index: Index, flags, ids, r: float) -> np.ndarray:
     """updateIndexRnn (update.cuh:449): -> the result count of every query op."""
     return index.update_run(flags, ids, r)[0]

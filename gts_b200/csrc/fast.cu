@@ -605,7 +605,11 @@ constexpr uint32_t kStagedUnused = 0xffffffffu;
 //              (shared-memory atomics only) and written to the queries'
 //              candidate lists once per item, one global atomic per query.
 // The CTA synchronises only between items.
-template <int CG>
+//
+// KH > 0 (k <= KH): each epilogue thread keeps its k smallest upper bounds in
+// registers (slots k..KH-1 hold -FLT_MAX and are never the largest); KH = 0:
+// in shared memory, k per thread.
+template <int CG, int KH>
 __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
 {
     constexpr int NT = 128 * CG;   // epilogue threads
@@ -620,7 +624,7 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
     const uint32_t rec_pad = (fs.rec_bytes + 1023u) & ~1023u;
     unsigned char *B0 = base + arec_pad;
     float *heap = reinterpret_cast<float *>(B0 + kFS * rec_pad);
-    FastCtl &ctl = *reinterpret_cast<FastCtl *>(heap + NT * a.k);
+    FastCtl &ctl = *reinterpret_cast<FastCtl *>(heap + (KH > 0 ? 0 : NT * a.k));
     FastStaged *stg = reinterpret_cast<FastStaged *>(&ctl + 1);
     const int st_cap = a.st_cap;
 
@@ -743,7 +747,13 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
             const int qi = inf.x;
             const float q2 = __int_as_float(inf.y), qn = __int_as_float(inf.z);
             const float cr = 2.f * kEpsR * qn;
-            for (int i = 0; i < k; i++) heap[i * NT + t] = FLT_MAX;
+            float hreg[KH > 0 ? KH : 1];
+            if constexpr (KH > 0) {
+#pragma unroll
+                for (int h = 0; h < KH; h++) hreg[h] = h < k ? FLT_MAX : -FLT_MAX;
+            } else {
+                for (int i = 0; i < k; i++) heap[i * NT + t] = FLT_MAX;
+            }
             // the query's bound as published so far (its seed, tightened by
             // items of the same tile that finished earlier)
             const float seed = qi >= 0 ? __int_as_float(*(volatile const int *)(a.r2_bits + qi)) : FLT_MAX;
@@ -854,11 +864,21 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                             gsl++;
                         }
                         if (ub < R2) {   // replace the largest of the k kept bounds
-                            heap[hidx * NT + t] = ub;
-                            float mx = -1.f;
-                            for (int h = 0; h < k; h++) {
-                                const float hv = heap[h * NT + t];
-                                if (hv > mx) { mx = hv; hidx = h; }
+                            float mx = -FLT_MAX;
+                            if constexpr (KH > 0) {
+                                int mi = 0;
+#pragma unroll
+                                for (int h = 0; h < KH; h++) {
+                                    if (h == hidx) hreg[h] = ub;
+                                    if (hreg[h] > mx) { mx = hreg[h]; mi = h; }
+                                }
+                                hidx = mi;
+                            } else {
+                                heap[hidx * NT + t] = ub;
+                                for (int h = 0; h < k; h++) {
+                                    const float hv = heap[h * NT + t];
+                                    if (hv > mx) { mx = hv; hidx = h; }
+                                }
                             }
                             hmx = mx;
                             R2 = fminf(R2, mx);
@@ -1115,13 +1135,13 @@ static FastCfg fast_default_cfg(const gts_index *idx, int k)
     return FastCfg{idx->mlp_ready && k >= 16, fast_cg(k), 16};
 }
 
-template <int CG>
+template <int CG, int KH>
 static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
 {
     const uint32_t arec_pad = (a.fs.arec_bytes + 1023u) & ~1023u;
     const uint32_t rec_pad = (a.fs.rec_bytes + 1023u) & ~1023u;
-    const size_t fixed = 1024 + (size_t)arec_pad + kFS * (size_t)rec_pad + sizeof(float) * 128 * CG * (size_t)a.k +
-                         sizeof(FastCtl) + 64;
+    const size_t heap = KH > 0 ? 0 : sizeof(float) * 128 * CG * (size_t)a.k;
+    const size_t fixed = 1024 + (size_t)arec_pad + kFS * (size_t)rec_pad + heap + sizeof(FastCtl) + 64;
     int dev = 0, optin = 0;
     GTS_CUDA_TRY(cudaGetDevice(&dev));
     GTS_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -1133,18 +1153,26 @@ static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
         return GTS_ERR_INVALID;
     }
     const size_t smem = fixed + sizeof(FastStaged) * (size_t)b.st_cap;
-    GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_tile<CG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_fast_tile<CG><<<grid, 128 * CG + 32, smem, st>>>(b);
+    GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_tile<CG, KH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_fast_tile<CG, KH><<<grid, 128 * CG + 32, smem, st>>>(b);
     GTS_CUDA_TRY(cudaGetLastError());
     return GTS_OK;
 }
 
 static int launch_fast_tile(const FastTileArgs &a, int cg, int grid, cudaStream_t st)
 {
+    // k <= 8: the k kept bounds live in registers
+    if (a.k <= 8) {
+        switch (cg) {
+        case 4: return launch_fast_tile_cg<4, 8>(a, grid, st);
+        case 2: return launch_fast_tile_cg<2, 8>(a, grid, st);
+        default: return launch_fast_tile_cg<1, 8>(a, grid, st);
+        }
+    }
     switch (cg) {
-    case 4: return launch_fast_tile_cg<4>(a, grid, st);
-    case 2: return launch_fast_tile_cg<2>(a, grid, st);
-    default: return launch_fast_tile_cg<1>(a, grid, st);
+    case 4: return launch_fast_tile_cg<4, 0>(a, grid, st);
+    case 2: return launch_fast_tile_cg<2, 0>(a, grid, st);
+    default: return launch_fast_tile_cg<1, 0>(a, grid, st);
     }
 }
 

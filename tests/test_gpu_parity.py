@@ -140,6 +140,29 @@ def test_plain_thread_counts_agree_and_autotuner_picks_one(oracle):
     np.testing.assert_array_equal(counts[:200], bc)
 
 
+def test_v1_entry_points(oracle, tmp_path):
+    """searchIndexKnn / searchIndexRnn (the reference's v1 multi-query
+    search): flat id/distance arrays, count + prefix layout, cost file."""
+    rows = _data(2, 3000, 10, 23)
+    ds = oracle.Dataset(2, rows)
+    q = G.query_ids(3000, 40, 24)
+    r = float(np.float32(G.quantile_radius(2, 0.01, 20000, 25, rows=rows)))
+    bk, bi, bd = oracle.knn_brute(ds, q, 5)
+    bc = oracle.range_brute(ds, q, r)
+    cost = tmp_path / "cost.txt"
+    with gts.indexConstru(rows, 2, max_h=4) as idx:
+        ids, dis = gts.searchIndexKnn(idx, q, 5, fcost=str(cost))
+        np.testing.assert_array_equal(ids, bi.reshape(-1))
+        np.testing.assert_array_equal(dis, bd.reshape(-1))
+        assert cost.read_text() == "".join("%f " % v for v in bk)
+        cost.unlink()
+        counts, prefix, rid, rdis = gts.searchIndexRnn(idx, q, r, fcost=str(cost))
+    np.testing.assert_array_equal(counts, bc)
+    np.testing.assert_array_equal(prefix, np.concatenate([[0], np.cumsum(bc)[:-1]]))
+    assert len(rid) == len(rdis) == bc.sum()
+    assert cost.read_text() == "".join("%d " % v for v in bc)
+
+
 def test_update_equals_oracle(oracle):
     rows = _data(2, 1500, 10, 11)
     ds = oracle.Dataset(2, rows)
