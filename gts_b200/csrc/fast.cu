@@ -98,6 +98,21 @@ __global__ void __launch_bounds__(kFB) k_fast_layout(const int *__restrict__ per
     }
 }
 
+// One CTA per block: the FP32 rows of its slots, in slot order (row stride
+// kp, zeros past dim and in padding slots), so the seed and the exact
+// recheck read a block's rows from one contiguous range.
+__global__ void __launch_bounds__(kFB) k_fast_prows(int dim, int kp, const float *__restrict__ rows,
+                                                   const int *__restrict__ ids, float *__restrict__ prow)
+{
+    const int b = blockIdx.x, t = threadIdx.x;
+    for (int r = 0; r < kFB; r++) {
+        const int slot = b * kFB + r;
+        const int id = ids[slot];
+        for (int j = t; j < kp; j += kFB)
+            prow[(size_t)slot * kp + j] = (id >= 0 && j < dim) ? rows[(size_t)id * dim + j] : 0.f;
+    }
+}
+
 // One CTA per block; thread t = slot t of the block.
 __global__ void __launch_bounds__(kFB) k_fast_prep(int dim, const float *__restrict__ rows,
                                                    unsigned char *__restrict__ recs, FastShape fs, FastSummary bs)
@@ -265,42 +280,39 @@ __global__ void __launch_bounds__(128) k_fast_arec(const float *__restrict__ row
 // One CTA per query: the k-th smallest FP32 squared distance inside the
 // query's own block (the query is one of its objects), widened past every
 // rounding difference to the reference's value, lowers the query's bound.
-// One warp per object row (coalesced), four rows in flight per warp.
+// The block's rows are read from the slot-ordered copy (one contiguous
+// 128 x kp range): one warp per row, lane l holding dimensions 4l..4l+3,
+// eight rows in flight per warp.
 __global__ void __launch_bounds__(128) k_fast_seed(const float *__restrict__ rows, const int *__restrict__ qids,
-                                                   FastSummary bs, int dim, int k, int *__restrict__ r2_bits)
+                                                   FastSummary bs, int dim, int kp, int k, int *__restrict__ r2_bits)
 {
     __shared__ float v[kFB];
     const int q = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int qid = qids[q];
     const int base = bs.pos[qid] / kFB * kFB;
-    const int cnt = __syncthreads_count(bs.ids[base + t] >= 0);
+    const int cnt = __syncthreads_count(bs.ids[base + t] >= 0);   // valid slots come first
     if (cnt < k) return;
     const float *qr = rows + (size_t)qid * dim;
-    float qv[kFMaxKp / 32];
+    const bool act = 4 * lane < kp;   // kp <= 128
+    float qv[4];
 #pragma unroll
-    for (int u = 0; u < kFMaxKp / 32; u++) qv[u] = lane + 32 * u < dim ? qr[lane + 32 * u] : 0.f;
-    for (int i0 = 0; i0 < 32; i0 += 4) {
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        int id[4];
+    for (int e = 0; e < 4; e++) qv[e] = (act && 4 * lane + e < dim) ? qr[4 * lane + e] : 0.f;
+    const float *pb = bs.prow + (size_t)base * kp + 4 * lane;
+    for (int i0 = 0; i0 < 32; i0 += 8) {
+        float acc[8];
 #pragma unroll
-        for (int r = 0; r < 4; r++) id[r] = bs.ids[base + warp * 32 + i0 + r];
-#pragma unroll
-        for (int u = 0; u < kFMaxKp / 32; u++) {
-            const int d = lane + 32 * u;
-            if (d < dim) {
-#pragma unroll
-                for (int r = 0; r < 4; r++) {
-                    if (id[r] >= 0) {
-                        const float e = rows[(size_t)id[r] * dim + d] - qv[u];
-                        acc[r] = fmaf(e, e, acc[r]);
-                    }
-                }
-            }
+        for (int r = 0; r < 8; r++) {
+            const int row = warp * 32 + i0 + r;
+            float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (act && row < cnt) o = *reinterpret_cast<const float4 *>(pb + (size_t)row * kp);
+            const float e0 = o.x - qv[0], e1 = o.y - qv[1], e2 = o.z - qv[2], e3 = o.w - qv[3];
+            acc[r] = fmaf(e3, e3, fmaf(e2, e2, fmaf(e1, e1, e0 * e0)));
         }
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
+        for (int r = 0; r < 8; r++) {
             const float s = warp_sum(acc[r]);
-            if (lane == 0) v[warp * 32 + i0 + r] = id[r] >= 0 ? s : FLT_MAX;
+            const int row = warp * 32 + i0 + r;
+            if (lane == 0) v[row] = row < cnt ? s : FLT_MAX;
         }
     }
     __syncthreads();
@@ -315,9 +327,9 @@ __global__ void __launch_bounds__(128) k_fast_seed(const float *__restrict__ row
             __syncthreads();
         }
     }
-    // FP32 sum of 128 non-negative terms (4 per lane, then a 32-lane tree):
-    // relative error < 2^-19 against the reference's FP64 sum of the same
-    // FP32 differences
+    // FP32 sum of at most 128 non-negative terms (4 per lane, then a 32-lane
+    // tree): relative error < 2^-19 against the reference's FP64 sum of the
+    // same FP32 differences
     if (t == 0) atomicMin(&r2_bits[q], __float_as_int(v[k - 1] * (1.f + 3e-5f)));
 }
 
@@ -944,11 +956,19 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
 // One CTA (4 warps) per query.  The bound drops to the k-th smallest
 // candidate upper bound (the candidates are distinct objects); every
 // candidate whose lower bound is within it gets its reference-arithmetic
-// distance, one warp per candidate; top k by (distance, id).  Queries that
-// cannot be answered from their list (it overflowed, or fewer than k exact
-// values lie inside the bound because a learned seed was too small) are
-// listed in overflow.
+// distance; top k by (distance, id).  Queries that cannot be answered from
+// their list (it overflowed, or fewer than k exact values lie inside the
+// bound because a learned seed was too small) are listed in overflow.
+//
+// The reference value of a candidate is a sequential F64 sum of
+// pow(o_j - q_j, 2) over j: in batches of kFinB candidates, the four warps
+// evaluate the pow terms (coalesced rows) into shared memory and lane c of
+// warp 0 adds candidate c's terms in j order, so the sums of a batch run
+// side by side, each bit-identical to the sequential one.
+constexpr int kFinB = 16;
+
 __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ rows, int dim, int num,
+                                                    const float *__restrict__ prow, int kp,
                                                     const int *__restrict__ ids_of_slot, int nslots,
                                                     const int *__restrict__ qids, int k, int infi_dis,
                                                     const int *__restrict__ cand_pos,
@@ -961,10 +981,16 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
 {
     __shared__ double cd[kFCand];
     __shared__ int cid[kFCand];
-    __shared__ float ubs[kFCand];
     __shared__ int cl[kFCand];
-    __shared__ double tbuf[4][kFMaxKp];
+    // the upper bounds (dead once the bound is set) share their space with the
+    // pow terms; +1 double per row: lane c's reads of column j miss each
+    // other's banks
+    constexpr int kTermsBytes = kFinB * (kFMaxKp + 1) * 8;
+    __shared__ __align__(16) unsigned char scratch[kTermsBytes > 4 * kFCand ? kTermsBytes : 4 * kFCand];
+    float *ubs = reinterpret_cast<float *>(scratch);
+    double(*terms)[kFMaxKp + 1] = reinterpret_cast<double(*)[kFMaxKp + 1]>(scratch);
     __shared__ int ns;
+    __shared__ float kub;
     const int q = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int qid = qids[q];
     const int cnt = cand_cnt[q];
@@ -974,23 +1000,34 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
     }
     float R2 = __int_as_float(r2_bits[q]);
     if (cnt >= k && cnt <= 128) {
-        // k-th smallest upper bound by rank: thread t counts the values
-        // below its own (ties ordered by index)
-        if (t < cnt) ubs[t] = cand_ub[(size_t)q * kFCand + t];
-        if (t == 0) ns = 0x7f800000;
-        __syncthreads();
-        if (t < cnt) {
-            const float v = ubs[t];
-            int rank = 0;
-            for (int i = 0; i < cnt; i++) {
-                const float x = ubs[i];
-                rank += (x < v) || (x == v && i < t);
+        // k-th smallest upper bound: warp 0 holds four per lane and takes
+        // out the smallest k - 1 times (one occurrence each)
+        if (warp == 0) {
+            float v[4];
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                const int i = lane + 32 * m;
+                v[m] = i < cnt ? cand_ub[(size_t)q * kFCand + i] : INFINITY;
             }
-            if (rank == k - 1) ns = __float_as_int(v);
+            float mn = INFINITY;
+            for (int it = 0; it < k; it++) {
+                const float lm = fminf(fminf(v[0], v[1]), fminf(v[2], v[3]));
+                mn = lm;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+                if (it == k - 1) break;
+                const unsigned own = __ballot_sync(0xffffffffu, lm == mn);
+                if (lane == __ffs(own) - 1) {
+                    if (v[0] == mn) v[0] = INFINITY;
+                    else if (v[1] == mn) v[1] = INFINITY;
+                    else if (v[2] == mn) v[2] = INFINITY;
+                    else v[3] = INFINITY;
+                }
+            }
+            if (lane == 0) kub = mn;
         }
         __syncthreads();
-        R2 = fminf(R2, __int_as_float(ns));
-        __syncthreads();
+        R2 = fminf(R2, kub);
     } else if (cnt >= k) {
         int p2 = 1;
         while (p2 < cnt) p2 <<= 1;
@@ -1017,20 +1054,62 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
         if (slot < 0 || slot >= nslots) continue;
         const int id = ids_of_slot[slot];
         if (id < 0 || id >= num) continue;
-        cl[atomicAdd(&ns, 1)] = id;
+        cl[atomicAdd(&ns, 1)] = slot;
     }
     __syncthreads();
     const int n = ns;
     const float *qrow = rows + (size_t)qid * dim;
-    for (int i = warp; i < n; i += 4) {
-        const int id = cl[i];
-        const double d = id == qid ? 0.0 : warp_dist_l2_f64(rows + (size_t)id * dim, qrow, dim, lane, tbuf[warp]);
-        if (lane == 0) {
-            cd[i] = d;
-            cid[i] = id;
+    for (int b0 = 0; b0 < n; b0 += kFinB) {
+        const int nb = min(kFinB, n - b0);
+        for (int c = warp; c < nb; c += 4) {
+            const float *orow = prow + (size_t)cl[b0 + c] * kp;
+            for (int j = lane; j < dim; j += 32) terms[c][j] = pow(orow[j] - qrow[j], 2);
         }
+        __syncthreads();
+        if (warp == 0 && lane < nb) {
+            const int id = ids_of_slot[cl[b0 + lane]];
+            double r = 0.0;
+#pragma unroll 4
+            for (int j = 0; j < dim; j++) r += terms[lane][j];
+            cd[b0 + lane] = id == qid ? 0.0 : pow(r, 0.5);
+            cid[b0 + lane] = id;
+        }
+        __syncthreads();
     }
     if (t == 0 && stats) atomicAdd(&stats[2], (unsigned long long)n);
+    // every object whose d^2 is within the bound is a candidate, and the
+    // reference value differs from d^2 by < 1e-6 relative: the answer is
+    // exact once k candidates have reference values inside R2 (1 - 1e-6)
+    const double lim = (double)R2 * (1.0 - 1e-6);
+    if (n <= 32) {
+        // rank of each candidate by (distance, id) within warp 0
+        if (warp != 0) return;
+        const double d = lane < n ? cd[lane] : DBL_MAX;
+        const int id = lane < n ? cid[lane] : 0x7fffffff;
+        int rank = 0;
+        for (int j = 0; j < n; j++) {
+            const double dj = __shfl_sync(0xffffffffu, d, j);
+            const int ij = __shfl_sync(0xffffffffu, id, j);
+            rank += (dj < d) || (dj == d && ij < id);
+        }
+        const bool top = lane < n && rank < k;
+        const int within = __popc(__ballot_sync(0xffffffffu, top && d * d <= lim));
+        if (within < k && within < num) {
+            if (lane == 0) overflow[atomicAdd(n_overflow, 1)] = q;
+            return;
+        }
+        if (top) {
+            if (ids) ids[(size_t)q * k + rank] = id;
+            if (dists) dists[(size_t)q * k + rank] = (float)d;
+            if (rank == k - 1) kth[q] = (float)d;
+        }
+        for (int j = n + lane; j < k; j += 32) {
+            if (ids) ids[(size_t)q * k + j] = -1;
+            if (dists) dists[(size_t)q * k + j] = (float)infi_dis;
+        }
+        if (n < k && lane == 0) kth[q] = (float)infi_dis;
+        return;
+    }
     int p2 = 1;
     while (p2 < n) p2 <<= 1;
     for (int i = n + t; i < p2; i += 128) {
@@ -1055,21 +1134,17 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
         }
     }
     if (t == 0) {
-        // every object whose d^2 is within the bound is a candidate, and the
-        // reference value differs from d^2 by < 1e-6 relative: the answer is
-        // exact once k candidates have reference values inside R2 (1 - 1e-6)
-        const double lim = (double)R2 * (1.0 - 1e-6);
         int within = 0;
         for (int i = 0; i < n && i < k; i++) within += cd[i] * cd[i] <= lim;
-        if (within < k && within < num) {
-            overflow[atomicAdd(n_overflow, 1)] = q;
-            return;
-        }
-        kth[q] = n >= k ? (float)cd[k - 1] : (float)infi_dis;
-        for (int j = 0; j < k; j++) {
-            if (ids) ids[(size_t)q * k + j] = j < n ? cid[j] : -1;
-            if (dists) dists[(size_t)q * k + j] = j < n ? (float)cd[j] : (float)infi_dis;
-        }
+        if (within < k && within < num) overflow[atomicAdd(n_overflow, 1)] = q;
+        else kth[q] = n >= k ? (float)cd[k - 1] : (float)infi_dis;
+        ns = within < k && within < num ? -1 : 0;
+    }
+    __syncthreads();
+    if (ns < 0) return;
+    for (int j = t; j < k; j += 128) {
+        if (ids) ids[(size_t)q * k + j] = j < n ? cid[j] : -1;
+        if (dists) dists[(size_t)q * k + j] = j < n ? (float)cd[j] : (float)infi_dis;
     }
 }
 
@@ -1201,6 +1276,7 @@ static int fast_prepare(gts_index *idx, cudaStream_t st)
     k_fast_layout<<<nb, kFB, 0, st>>>(ord.perm, ord.blk_l, ord.blk_r, bs.ids, bs.pos);
     GTS_CUDA_TRY(cudaMemcpyAsync(bs.sb_b0, ord.sb_b0, sizeof(int) * (nsb + 1), cudaMemcpyDeviceToDevice, st));
     k_fast_prep<<<nb, kFB, 0, st>>>(idx->dim, idx->rows, recs, fs, bs);
+    k_fast_prows<<<nb, kFB, 0, st>>>(idx->dim, fs.kp, idx->rows, bs.ids, bs.prow);
     k_fast_sbprep<<<nsb, 256, 0, st>>>(idx->dim, idx->rows, fs, bs);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -1299,7 +1375,7 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     idx->kernel_launches++;
     // the certified own-block seed; with a learned radius the smaller of the
     // two is used, and queries it under-predicts are answered again
-    k_fast_seed<<<qnum, 128, 0, st>>>(idx->rows, d_qids, bs, idx->dim, k, r.r2);
+    k_fast_seed<<<qnum, 128, 0, st>>>(idx->rows, d_qids, bs, idx->dim, fs.kp, k, r.r2);
     idx->kernel_launches++;
     const size_t need_smem = sizeof(float) * (size_t)fs.kp * (kFT + kFChunk);
     GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_sb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
@@ -1342,7 +1418,7 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
         GTS_CUDA_TRY(cudaEventRecordWithFlags(idx->fev[1], st, capturing ? cudaEventRecordExternal : 0));
     k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 1ull);
     idx->kernel_launches++;
-    k_fast_final<<<qnum, 128, 0, st>>>(idx->rows, idx->dim, idx->num, bs.ids, nb * kFB, d_qids, k,
+    k_fast_final<<<qnum, 128, 0, st>>>(idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k,
                                         idx->params.infi_dis, r.cpos, r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids,
                                         d_dists, d_fail, r.ctr, idx->d_stats);
     idx->kernel_launches++;

@@ -50,6 +50,7 @@ struct FastSummary {
     int *pos;                       // [num] object id -> slot
     float *sb_cen, *sb_c2, *sb_rad; // [nsb][kp], [nsb], [nsb]
     int *sb_b0;                     // [nsb + 1] first block of each superblock
+    float *prow;                    // [nb * kFB][kp] FP32 rows in slot order (zero padding)
 };
 
 inline size_t fast_rec_region(const FastShape &fs, int nb)
@@ -60,7 +61,7 @@ inline size_t fast_rec_region(const FastShape &fs, int nb)
 // Byte offsets of the summary arrays after the records, each 256-byte
 // aligned (the pruning kernels read centres as float4).
 struct FastSummaryOffsets {
-    size_t cen, c2, rad, ids, pos, sb_cen, sb_c2, sb_rad, sb_b0, end;
+    size_t cen, c2, rad, ids, pos, sb_cen, sb_c2, sb_rad, sb_b0, prow, end;
 };
 
 inline FastSummaryOffsets fast_summary_offsets(const FastShape &fs, int nb, int nsb, int n)
@@ -77,6 +78,7 @@ inline FastSummaryOffsets fast_summary_offsets(const FastShape &fs, int nb, int 
     o.sb_c2 = take(sizeof(float) * (size_t)nsb);
     o.sb_rad = take(sizeof(float) * (size_t)nsb);
     o.sb_b0 = take(sizeof(int) * ((size_t)nsb + 1));
+    o.prow = take(sizeof(float) * (size_t)nb * kFB * fs.kp);
     o.end = off;
     return o;
 }
@@ -99,6 +101,7 @@ inline FastSummary fast_summary(unsigned char *recs, const FastShape &fs, int nb
     s.sb_c2 = (float *)(recs + o.sb_c2);
     s.sb_rad = (float *)(recs + o.sb_rad);
     s.sb_b0 = (int *)(recs + o.sb_b0);
+    s.prow = (float *)(recs + o.prow);
     return s;
 }
 
