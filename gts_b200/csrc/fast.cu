@@ -380,22 +380,26 @@ __device__ __forceinline__ void need_load_tile(const float *__restrict__ rows, c
     }
 }
 
-// Balls c0 .. c0+63 (those below cend) against the tile: bit i of the
-// result is set when some query of the tile can reach ball c0 + i within
-// its seed:  |q - c|_lo - radius <= sqrt(seed).  256 threads: each computes
+// Balls c0 .. c0+63 (those below cend; with a list, balls list[0 .. cend-1]
+// and c0 = 0) against the tile: bit i of the result is set when some query
+// of the tile can reach ball i of the chunk within its seed:
+// |q - c|_lo - radius <= sqrt(seed).  256 threads: each computes
 // 8 queries (4tq..4tq+3 and 64+4tq..64+4tq+3, so a quarter warp reads 128
 // consecutive bytes: no bank conflicts) x 4 balls of FP32 q.c.
 __device__ __forceinline__ uint64_t need_chunk(const float *__restrict__ cen, const float *__restrict__ c2, const float *__restrict__ rad,
-                               int c0, int cend, int kp, const float *Qs, float *Cs, NeedSmem &sm)
+                               int c0, int cend, const int *list, int kp, const float *Qs, float *Cs, NeedSmem &sm)
 {
     const int t = threadIdx.x;
-    __syncthreads();   // previous chunk's Cs / flags consumed
+    __syncthreads();   // previous chunk's Cs / flags consumed, list written
     // thread (bb, j4): 4 dimensions of ball bb; consecutive threads take
     // consecutive balls, so the shared-memory writes do not conflict
     for (int i = t; i < (kp / 4) * kFChunk; i += 256) {
         const int bb = i % kFChunk, j4 = i / kFChunk;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (c0 + bb < cend) v = *reinterpret_cast<const float4 *>(cen + (size_t)(c0 + bb) * kp + 4 * j4);
+        if (c0 + bb < cend) {
+            const int ball = list ? list[bb] : c0 + bb;
+            v = *reinterpret_cast<const float4 *>(cen + (size_t)ball * kp + 4 * j4);
+        }
         Cs[(4 * j4 + 0) * kFChunk + bb] = v.x;
         Cs[(4 * j4 + 1) * kFChunk + bb] = v.y;
         Cs[(4 * j4 + 2) * kFChunk + bb] = v.z;
@@ -403,9 +407,10 @@ __device__ __forceinline__ uint64_t need_chunk(const float *__restrict__ cen, co
     }
     if (t < kFChunk) {
         const bool ok = c0 + t < cend;
-        sm.c2s[t] = ok ? c2[c0 + t] : 0.f;
-        sm.cns[t] = ok ? sqrtf(c2[c0 + t]) * 1.000001f : 0.f;
-        sm.rads[t] = ok ? rad[c0 + t] : -1.f;
+        const int ball = ok ? (list ? list[t] : c0 + t) : 0;
+        sm.c2s[t] = ok ? c2[ball] : 0.f;
+        sm.cns[t] = ok ? sqrtf(c2[ball]) * 1.000001f : 0.f;
+        sm.rads[t] = ok ? rad[ball] : -1.f;
     }
     if (t < 2) sm.flags[t] = 0u;
     __syncthreads();
@@ -475,7 +480,7 @@ __global__ void __launch_bounds__(256) k_need_sb(const float *__restrict__ rows,
     float *Qs = nsm, *Cs = nsm + fs.kp * kFT;
     const int tile = blockIdx.x, ch = blockIdx.y;
     need_load_tile(rows, qids, arec, fs, dim, tile, r2_bits, Qs, sm);
-    const uint64_t m = need_chunk(bs.sb_cen, bs.sb_c2, bs.sb_rad, ch * kFChunk, nsb, fs.kp, Qs, Cs, sm);
+    const uint64_t m = need_chunk(bs.sb_cen, bs.sb_c2, bs.sb_rad, ch * kFChunk, nsb, nullptr, fs.kp, Qs, Cs, sm);
     if (threadIdx.x == 0) {
         sb_mask[(size_t)tile * nsbw + 2 * ch] = (uint32_t)m;
         if (2 * ch + 1 < nsbw) sb_mask[(size_t)tile * nsbw + 2 * ch + 1] = (uint32_t)(m >> 32);
@@ -483,8 +488,9 @@ __global__ void __launch_bounds__(256) k_need_sb(const float *__restrict__ rows,
 }
 
 // Blocks the tile needs, inside the superblocks it needs: CTA (tile, y)
-// takes every gridDim.y-th needed superblock; needed blocks are appended to
-// blist[tile][nbcap] (count in bcnt[tile]).
+// takes every gridDim.y-th needed superblock, gathers their blocks into
+// full chunks of kFChunk (superblocks hold 1..32 blocks) and appends the
+// needed ones to blist[tile][nbcap] (count in bcnt[tile]).
 __global__ void __launch_bounds__(256) k_need_blk(const float *__restrict__ rows, const int *__restrict__ qids,
                                                   const unsigned char *__restrict__ arec, FastShape fs, int dim,
                                                   FastSummary bs, const int *__restrict__ r2_bits,
@@ -494,8 +500,10 @@ __global__ void __launch_bounds__(256) k_need_blk(const float *__restrict__ rows
 {
     extern __shared__ __align__(16) float nsm[];
     __shared__ NeedSmem sm;
+    // two chunk lists: thread 0 reads chunk p's while chunk p + 1's is written
+    __shared__ int cblk[2][kFChunk];
     float *Qs = nsm, *Cs = nsm + fs.kp * kFT;
-    const int tile = blockIdx.x;
+    const int tile = blockIdx.x, t = threadIdx.x;
     // the superblocks of this CTA first, so a CTA with none returns early
     int mine = 0, seen = 0;
     for (int w = 0; w < nsbw; w++) {
@@ -507,6 +515,27 @@ __global__ void __launch_bounds__(256) k_need_blk(const float *__restrict__ rows
     if (mine == 0) return;
     need_load_tile(rows, qids, arec, fs, dim, tile, r2_bits, Qs, sm);
     unsigned long long tested = 0;
+    int fill = 0, p = 0;
+    int *dst = blist + (size_t)tile * nbcap;
+    auto run_chunk = [&]() {
+        const uint64_t m0 = need_chunk(bs.cen, bs.c2, bs.rad, 0, fill, cblk[p], fs.kp, Qs, Cs, sm);
+        if (t == 0) {
+            tested += (unsigned long long)fill;
+            uint64_t m = m0;
+            const int cnt = __popcll(m);
+            if (cnt) {
+                int at = atomicAdd(&bcnt[tile], cnt);
+                while (m) {
+                    const int i = __ffsll((long long)m) - 1;
+                    m &= m - 1;
+                    if (at < nbcap) dst[at] = cblk[p][i];
+                    at++;
+                }
+            }
+        }
+        fill = 0;
+        p ^= 1;
+    };
     seen = 0;
     for (int w = 0; w < nsbw; w++) {
         uint32_t word = sb_mask[(size_t)tile * nsbw + w];
@@ -514,27 +543,18 @@ __global__ void __launch_bounds__(256) k_need_blk(const float *__restrict__ rows
             const int s = w * 32 + __ffs(word) - 1;
             word &= word - 1;
             if (seen++ % gridDim.y != blockIdx.y) continue;
-            const int b0 = bs.sb_b0[s], b1 = bs.sb_b0[s + 1];
-            for (int c0 = b0; c0 < b1; c0 += kFChunk) {
-                uint64_t m = need_chunk(bs.cen, bs.c2, bs.rad, c0, b1, fs.kp, Qs, Cs, sm);
-                if (threadIdx.x == 0) {
-                    tested += (unsigned long long)min(kFChunk, b1 - c0);
-                    const int cnt = __popcll(m);
-                    if (cnt) {
-                        int at = atomicAdd(&bcnt[tile], cnt);
-                        int *dst = blist + (size_t)tile * nbcap;
-                        while (m) {
-                            const int i = __ffsll((long long)m) - 1;
-                            m &= m - 1;
-                            if (at < nbcap) dst[at] = c0 + i;
-                            at++;
-                        }
-                    }
-                }
+            const int b1 = bs.sb_b0[s + 1];
+            for (int b = bs.sb_b0[s]; b < b1;) {
+                const int take = min(b1 - b, kFChunk - fill);
+                if (t < take) cblk[p][fill + t] = b + t;
+                fill += take;
+                b += take;
+                if (fill == kFChunk) run_chunk();
             }
         }
     }
-    if (threadIdx.x == 0 && stats && tested) atomicAdd(&stats[7], tested);
+    if (fill > 0) run_chunk();
+    if (t == 0 && stats && tested) atomicAdd(&stats[7], tested);
 }
 
 // Work items: (tile, first list entry) per `item` needed blocks of a tile.
