@@ -128,10 +128,12 @@ def config_dict(args, world):
     return {"workload": f"gmm{args.n // 1000}k_d{args.dim}_l2_knn",
             "n": args.n, "dim": args.dim, "metric": "L2", "queries_per_gpu": args.queries,
             "k": args.k, "tree_order": 10, "max_size": 20, "max_h": args.max_h,
-            "form": args.form + ("" if args.form == "plain" else
+            "form": args.form + ("" if args.form != "fast" else
                                  (" (block-pruned bf16 filter)" if args.no_learn else
-                                  " (learned radius trained + block-pruned bf16 filter; the autotuner "
-                                  "decides per k whether the learned seed is used)")),
+                                  " (learned radius trained + block-pruned bf16 filter; " +
+                                  {"auto": "the autotuner decides per k whether the learned seed is used)",
+                                   "on": "learned seed forced on)",
+                                   "off": "learned seed forced off)"}[args.learned_seed])),
             "parallelism": f"query-sharded replicas x{world}",
             "l2_flush": "no (512 MB data set > 126 MB L2)"}
 
@@ -231,9 +233,9 @@ def run_gts(args):
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
     del d_rows
-    form = gts.FORM_FAST if args.form == "fast" else gts.FORM_PLAIN
+    form = {"fast": gts.FORM_FAST, "plain": gts.FORM_PLAIN, "plain-learned": gts.FORM_PLAIN_LEARNED}[args.form]
     learn = None
-    if args.form == "fast" and not args.no_learn:
+    if args.form in ("fast", "plain-learned") and not args.no_learn:
         # learned radius: 200,000 exact radii from the index itself, trained on
         # the device before the timed region
         torch.cuda.synchronize()
@@ -249,6 +251,11 @@ def run_gts(args):
     def step():
         idx.knn_device(d_q.data_ptr(), Q, k, d_kth.data_ptr(), form=form, stream=stream.cuda_stream)
 
+    if learn is not None and args.form == "fast" and args.learned_seed != "auto":
+        step()   # tunes the configuration for k, then the seed choice is pinned
+        torch.cuda.synchronize()
+        c = idx.fast_config(k)
+        idx.set_fast_config(k, args.learned_seed == "on", c["col_groups"], c["item_blocks"])
     clocks = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         step()
@@ -330,7 +337,7 @@ def run_gts(args):
     if os.path.exists(tpath):
         with open(tpath) as f:
             per_unit = json.load(f)
-    if args.form == "plain":
+    if args.form != "fast":
         # every leaf row and pivot row a query reads, plus its own row and result
         alg_bytes = 4 * d * (stats["objects"] + stats["pivots"]) + Q * (4 * d + 8 * k)
         achieved = alg_bytes / (launch_ms / 1e3) / 1e9
@@ -374,7 +381,7 @@ def run_gts(args):
     line = {"metric": "exact kNN queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32/f64" if args.form == "plain" else "bf16/f32/f64",
+            "dtype": "f32/f64" if args.form != "fast" else "bf16/f32/f64",
             "data": "synthetic (seeded Gaussian mixture; the paper's data sets are absent)",
             "config": config_dict(args, world), "build_s": build_s, "learned_radius": learn,
             "autotune": (idx.fast_config(k) if args.form == "fast"
@@ -398,7 +405,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["gts", "reference"], default="gts")
-    ap.add_argument("--form", choices=["fast", "plain"], default="fast")
+    ap.add_argument("--form", choices=["fast", "plain", "plain-learned"], default="fast",
+                    help="plain-learned: the plain traversal seeded by the trained radius")
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--dim", type=int, default=128)
     ap.add_argument("--queries", type=int, default=10_000)
@@ -409,6 +417,9 @@ def main():
     ap.add_argument("--no-learn", action="store_true",
                     help="fast form without the learned radius (own-block seeds only)")
     ap.add_argument("--train", type=int, default=200_000, help="learned-radius training samples")
+    ap.add_argument("--learned-seed", choices=["auto", "on", "off"], default="auto",
+                    help="fast form with a trained radius: let the autotuner choose the learned seed, "
+                         "or force it on / off (the other tuned settings are kept)")
     ap.add_argument("--profile", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()

@@ -982,9 +982,9 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
 //
 // The reference value of a candidate is a sequential F64 sum of
 // pow(o_j - q_j, 2) over j: in batches of kFinB candidates, the four warps
-// evaluate the pow terms (coalesced rows) into shared memory and lane c of
-// warp 0 adds candidate c's terms in j order, so the sums of a batch run
-// side by side, each bit-identical to the sequential one.
+// evaluate the terms (coalesced rows) into shared memory and lane c of warp 0
+// adds candidate c's terms in j order, so the sums of a batch run side by
+// side, each in the sequential order.
 constexpr int kFinB = 16;
 
 __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ rows, int dim, int num,
@@ -1079,28 +1079,72 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
     __syncthreads();
     const int n = ns;
     const float *qrow = rows + (size_t)qid * dim;
-    for (int b0 = 0; b0 < n; b0 += kFinB) {
-        const int nb = min(kFinB, n - b0);
-        for (int c = warp; c < nb; c += 4) {
-            const float *orow = prow + (size_t)cl[b0 + c] * kp;
-            for (int j = lane; j < dim; j += 32) terms[c][j] = pow(orow[j] - qrow[j], 2);
-        }
-        __syncthreads();
-        if (warp == 0 && lane < nb) {
-            const int id = ids_of_slot[cl[b0 + lane]];
-            double r = 0.0;
-#pragma unroll 4
-            for (int j = 0; j < dim; j++) r += terms[lane][j];
-            cd[b0 + lane] = id == qid ? 0.0 : pow(r, 0.5);
-            cid[b0 + lane] = id;
-        }
-        __syncthreads();
-    }
-    if (t == 0 && stats) atomicAdd(&stats[2], (unsigned long long)n);
     // every object whose d^2 is within the bound is a candidate, and the
     // reference value differs from d^2 by < 1e-6 relative: the answer is
     // exact once k candidates have reference values inside R2 (1 - 1e-6)
     const double lim = (double)R2 * (1.0 - 1e-6);
+    // Pass 0 (n <= 32) sums exact squares e * e (a float difference squared
+    // is exact in FP64) instead of pow(e, 2).  pow is within 2 ulp of the
+    // square, so over dim <= 128 terms the sequential sums differ by less
+    // than 2.9e-14 relative and the distances by less than 1.6e-14; with the
+    // margin delta = 1e-13 v the pass-0 values give the reference's float
+    // values, order and bound tests unless some value lies within delta of a
+    // float rounding midpoint, of another candidate's value or of the bound.
+    // Then (and for n > 32) pass 1 evaluates pow itself.
+    __shared__ int risky;
+    if (t == 0) risky = 0;
+    for (int pass = n <= 32 ? 0 : 1; pass < 2; pass++) {
+        for (int b0 = 0; b0 < n; b0 += kFinB) {
+            const int nb = min(kFinB, n - b0);
+            for (int c = warp; c < nb; c += 4) {
+                const float *orow = prow + (size_t)cl[b0 + c] * kp;
+                if (pass == 0) {
+                    for (int j = lane; j < dim; j += 32) {
+                        const double e = (double)(orow[j] - qrow[j]);
+                        terms[c][j] = e * e;
+                    }
+                } else {
+                    for (int j = lane; j < dim; j += 32) terms[c][j] = pow(orow[j] - qrow[j], 2);
+                }
+            }
+            __syncthreads();
+            if (warp == 0 && lane < nb) {
+                const int id = ids_of_slot[cl[b0 + lane]];
+                double r = 0.0;
+#pragma unroll 4
+                for (int j = 0; j < dim; j++) r += terms[lane][j];
+                const double v = id == qid ? 0.0 : pow(r, 0.5);
+                cd[b0 + lane] = v;
+                cid[b0 + lane] = id;
+                if (pass == 0 && v != 0.0) {
+                    // the float midpoints around (float)v must stay beyond delta
+                    const float f = __double2float_rn(v);
+                    const double fd = f;
+                    const double mhi = 0.5 * (fd + (double)__int_as_float(__float_as_int(f) + 1));
+                    const double mlo = 0.5 * (fd + (double)__int_as_float(__float_as_int(f) - 1));
+                    const double dl = v * 1e-13;
+                    const double v2 = v * v;
+                    if (!(f > 0.f && v - dl > mlo && v + dl < mhi) || fabs(v2 - lim) <= 3e-13 * lim) risky = 1;
+                }
+            }
+            __syncthreads();
+        }
+        if (pass == 1) break;
+        if (warp == 0) {
+            // near-ties: two values closer than their margins (exact zeros
+            // are exact in both sums)
+            const double d = lane < n ? cd[lane] : 0.0;
+            bool rk = false;
+            for (int j = 0; j < n; j++) {
+                const double dj = __shfl_sync(0xffffffffu, d, j);
+                if (lane < n && j != lane && !(d == 0.0 && dj == 0.0) && fabs(dj - d) <= (d + dj) * 1e-13) rk = true;
+            }
+            if (__any_sync(0xffffffffu, rk) && lane == 0) risky = 1;
+        }
+        __syncthreads();
+        if (!risky) break;
+    }
+    if (t == 0 && stats) atomicAdd(&stats[2], (unsigned long long)n);
     if (n <= 32) {
         // rank of each candidate by (distance, id) within warp 0
         if (warp != 0) return;

@@ -28,6 +28,7 @@
 // 454-456).  Deleted objects (update path) are skipped
 // (update.cuh:244).  Objects of every childless node are verified, at any
 // depth, so results equal the exact answer for every tree shape.
+#include <algorithm>
 #include <cfloat>
 #include <cstdio>
 #include "index.cuh"
@@ -596,21 +597,26 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
 
 // ---------------------------------------------------------------------------
 
-constexpr int kPlainTuneMin = 1024;
-constexpr int kPlainTuneSample = 256;
 constexpr int kPlainDefaultThreads = 256;
+
+// Persistent CTAs of k_search<NT> that fit on the device at once.
+template <int NT>
+static int search_resident()
+{
+    int dev = 0, nsm = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(k_search<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SearchSmem));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search<NT>, NT, sizeof(SearchSmem));
+    return nsm * (per_sm < 1 ? 1 : per_sm);
+}
 
 template <int NT>
 static int launch_search_nt(gts_index *idx, const SearchArgs &a, cudaStream_t st)
 {
     const size_t smem = sizeof(SearchSmem);
     GTS_CUDA_TRY(cudaFuncSetAttribute(k_search<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int dev = 0, nsm = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search<NT>, NT, smem);
-    if (per_sm < 1) per_sm = 1;
-    int grid = nsm * per_sm;
+    int grid = search_resident<NT>();
     if (grid > a.qnum) grid = a.qnum;
     k_search<NT><<<grid, NT, smem, st>>>(a);
     idx->kernel_launches++;
@@ -627,20 +633,25 @@ static int launch_search(gts_index *idx, const SearchArgs &a, int nt, cudaStream
     }
 }
 
-// Times 128 / 256 / 512 threads per query CTA on the batch's first
-// kPlainTuneSample queries (results identical; the full batch then runs with
-// the fastest).  Range-id mode is not tuned (its output offsets belong to
-// the whole batch): it takes the range-count choice.  A seeded kNN batch is
-// timed unseeded (the seeds' failure list belongs to the real run).
+// Times 128 / 256 / 512 threads per query CTA on the batch's leading queries
+// (results identical; the full batch then runs with the fastest).  The
+// sample is four times the most CTAs any candidate keeps resident, so the
+// timing is throughput rather than the latency of a few queries; batches
+// below twice the sample are not tuned (*best_nt = 0: the default runs).
+// Each candidate is warmed on one query first.  Range-id mode is not tuned
+// (its output offsets belong to the whole batch): it takes the range-count
+// choice.  A seeded kNN batch is timed unseeded (the seeds' failure list
+// belongs to the real run).
 static int plain_autotune(gts_index *idx, const SearchArgs &a, cudaStream_t st, int *best_nt)
 {
-    *best_nt = kPlainDefaultThreads;
+    *best_nt = 0;
     if (a.mode == kModeRangeIds) {
-        if (idx->plain_nt[kModeRangeCount]) *best_nt = idx->plain_nt[kModeRangeCount];
+        *best_nt = idx->plain_nt[kModeRangeCount];
         return GTS_OK;
     }
+    const int sample = 4 * std::max(search_resident<128>(), std::max(search_resident<256>(), search_resident<512>()));
+    if (a.qnum < 2 * sample) return GTS_OK;
     SearchArgs t = a;
-    t.qnum = kPlainTuneSample;
     t.seed_r2_bits = nullptr;
     cudaEvent_t e0, e1;
     GTS_CUDA_TRY(cudaEventCreate(&e0));
@@ -648,8 +659,9 @@ static int plain_autotune(gts_index *idx, const SearchArgs &a, cudaStream_t st, 
     float best = 3.0e38f;
     int rc = GTS_OK;
     const int cand[3] = {128, 256, 512};
-    for (int rep = 0; rep < 2 && rc == GTS_OK; rep++)   // first pass warms caches and modules
+    for (int rep = 0; rep < 2 && rc == GTS_OK; rep++)   // rep 0: one query per candidate (module load, caches)
         for (int c : cand) {
+            t.qnum = rep == 0 ? 1 : sample;
             cudaMemsetAsync(idx->d_counter, 0, sizeof(int), st);
             cudaEventRecord(e0, st);
             if ((rc = launch_search(idx, t, c, st))) break;
@@ -716,14 +728,13 @@ static int run_search(gts_index *idx, SearchArgs &a, cudaStream_t st)
     GTS_CUDA_TRY(cudaMemsetAsync(idx->d_counter, 0, sizeof(int), st));
     GTS_CUDA_TRY(cudaMemsetAsync(idx->d_status, 0, sizeof(int), st));
     if (!idx->keep_stats) GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, kStatsN * sizeof(unsigned long long), st));
-    // threads per query CTA: tuned per search mode on the first batch of at
-    // least kPlainTuneMin queries (each candidate on the same leading
-    // kPlainTuneSample queries, CUDA events), else the tuned or default value
+    // threads per query CTA: tuned per search mode on the first batch large
+    // enough for plain_autotune's sample, else the tuned or default value
     int nt = idx->plain_nt[a.mode];
-    if (!nt && a.qnum >= kPlainTuneMin && !idx->keep_stats) {
+    if (!nt && !idx->keep_stats) {
         int rc = plain_autotune(idx, a, st, &nt);
         if (rc) return rc;
-        idx->plain_nt[a.mode] = nt;
+        if (a.mode != kModeRangeIds) idx->plain_nt[a.mode] = nt;
     }
     if (!nt) nt = kPlainDefaultThreads;
     int rc = launch_search(idx, a, nt, st);

@@ -153,11 +153,12 @@ int gts_fast_autotune_reset(gts_index *idx);
 
 /* No counterpart in the reference (search_v2.cuh: THREAD_NUM per query
  * block).  Threads per query CTA of the plain traversal for one search mode
- * (0 kNN, 1 range count, 2 range ids).  The first batch of at least 1024
- * queries of a mode times 128 / 256 / 512 on its first 256 queries and
- * keeps the fastest (the answers do not depend on it); *threads = 0 means
- * not tuned yet (256 is used).  _set pins it (128, 256, 512; 0 = tune
- * again). */
+ * (0 kNN, 1 range count, 2 range ids).  The first batch of a mode with at
+ * least twice the tuning sample (four times the most query CTAs resident at
+ * once, about 1,800 on a B200) times 128 / 256 / 512 on its leading sample
+ * and keeps the fastest (the answers do not depend on it); range ids take
+ * the range-count choice.  *threads = 0 means not tuned yet (256 is used).
+ * _set pins it (128, 256, 512; 0 = tune again). */
 int gts_plain_threads(const gts_index *idx, int mode, int *threads);
 int gts_plain_threads_set(gts_index *idx, int mode, int threads);
 

@@ -109,3 +109,20 @@ def test_graph_replay_equals_direct_launches(oracle):
         assert idx.fast_graphs() - n0 == 5
     bk, bi, _ = oracle.knn_brute(ds, q1, 8)
     np.testing.assert_array_equal(direct[0][1], bi)
+
+
+def test_fast_exact_ties_from_duplicate_rows(oracle):
+    """Every row present twice: each query's candidates come in equal-distance
+    pairs, so the recheck cannot certify the exact-square sums and evaluates
+    the reference's pow terms; ties are broken by id."""
+    base = G.gmm_rows(4000, 64, 10, 0.3, seed=61)
+    rows = np.concatenate([base, base])
+    ds = oracle.Dataset(2, rows)
+    q = G.query_ids(len(rows), 300, seed=62)
+    with gts.Index(rows, 2, max_h=4) as idx:
+        for k in (2, 7, 16):
+            kth, ids, dis = idx.knn(q, k, form=gts.FORM_FAST, return_ids=True)
+            bk, bi, bd = oracle.knn_brute(ds, q, k)
+            np.testing.assert_array_equal(ids, bi, err_msg=f"k={k}")
+            np.testing.assert_array_equal(kth, bk, err_msg=f"k={k}")
+            np.testing.assert_array_equal(dis, bd, err_msg=f"k={k}")

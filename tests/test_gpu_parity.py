@@ -111,10 +111,10 @@ def test_range_ids(oracle):
 
 def test_plain_thread_counts_agree_and_autotuner_picks_one(oracle):
     """Every threads-per-query-CTA choice of the plain traversal gives the
-    same exact answers; a batch of 1024+ queries tunes the choice."""
+    same exact answers; a large enough batch tunes the choice."""
     rows = _data(2, 12000, 24, 17)
     ds = oracle.Dataset(2, rows)
-    q = G.query_ids(12000, 1100, 18)
+    q = G.query_ids(12000, 6000, 18)
     r = float(np.float32(G.quantile_radius(2, 0.005, 30000, 19, rows=rows)))
     bk, bi, bd = oracle.knn_brute(ds, q[:200], 8)
     bc = oracle.range_brute(ds, q[:200], r)
