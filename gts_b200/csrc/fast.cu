@@ -640,6 +640,7 @@ constexpr uint32_t kStagedUnused = 0xffffffffu;
 //
 // KH > 0 (k <= KH): each epilogue thread keeps its k smallest upper bounds in
 // registers (slots k..KH-1 hold -FLT_MAX and are never the largest); KH = 0:
+// as a binary max-heap
 // in shared memory, k per thread.
 template <int CG, int KH>
 __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
@@ -906,11 +907,25 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                                 }
                                 hidx = mi;
                             } else {
-                                heap[hidx * NT + t] = ub;
-                                for (int h = 0; h < k; h++) {
-                                    const float hv = heap[h * NT + t];
-                                    if (hv > mx) { mx = hv; hidx = h; }
+                                // binary max-heap in shared memory: the root
+                                // (the largest kept bound) is replaced and
+                                // sifted down, log2(k) levels
+                                int i = 0;
+                                for (;;) {
+                                    const int l = 2 * i + 1;
+                                    if (l >= k) break;
+                                    float cv = heap[l * NT + t];
+                                    int c = l;
+                                    if (l + 1 < k) {
+                                        const float rv = heap[(l + 1) * NT + t];
+                                        if (rv > cv) { cv = rv; c = l + 1; }
+                                    }
+                                    if (cv <= ub) break;
+                                    heap[i * NT + t] = cv;
+                                    i = c;
                                 }
+                                heap[i * NT + t] = ub;
+                                mx = heap[t];
                             }
                             hmx = mx;
                             R2 = fminf(R2, mx);
@@ -1083,17 +1098,20 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
     // reference value differs from d^2 by < 1e-6 relative: the answer is
     // exact once k candidates have reference values inside R2 (1 - 1e-6)
     const double lim = (double)R2 * (1.0 - 1e-6);
-    // Pass 0 (n <= 32) sums exact squares e * e (a float difference squared
+    // Pass 0 sums exact squares e * e (a float difference squared
     // is exact in FP64) instead of pow(e, 2).  pow is within 2 ulp of the
     // square, so over dim <= 128 terms the sequential sums differ by less
     // than 2.9e-14 relative and the distances by less than 1.6e-14; with the
     // margin delta = 1e-13 v the pass-0 values give the reference's float
     // values, order and bound tests unless some value lies within delta of a
     // float rounding midpoint, of another candidate's value or of the bound.
-    // Then (and for n > 32) pass 1 evaluates pow itself.
+    // Then pass 1 evaluates pow itself.  More than 32 candidates are sorted
+    // by (distance, id) here (bitonic), so near-ties are neighbours.
     __shared__ int risky;
     if (t == 0) risky = 0;
-    for (int pass = n <= 32 ? 0 : 1; pass < 2; pass++) {
+    int p2 = 1;
+    while (p2 < n) p2 <<= 1;
+    for (int pass = 0; pass < 2; pass++) {
         for (int b0 = 0; b0 < n; b0 += kFinB) {
             const int nb = min(kFinB, n - b0);
             for (int c = warp; c < nb; c += 4) {
@@ -1129,20 +1147,48 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
             }
             __syncthreads();
         }
-        if (pass == 1) break;
-        if (warp == 0) {
-            // near-ties: two values closer than their margins (exact zeros
-            // are exact in both sums)
-            const double d = lane < n ? cd[lane] : 0.0;
-            bool rk = false;
-            for (int j = 0; j < n; j++) {
-                const double dj = __shfl_sync(0xffffffffu, d, j);
-                if (lane < n && j != lane && !(d == 0.0 && dj == 0.0) && fabs(dj - d) <= (d + dj) * 1e-13) rk = true;
+        // near-ties: two values closer than their margins (exact zeros are
+        // exact in both sums)
+        if (n <= 32) {
+            if (pass == 0 && warp == 0) {
+                const double d = lane < n ? cd[lane] : 0.0;
+                bool rk = false;
+                for (int j = 0; j < n; j++) {
+                    const double dj = __shfl_sync(0xffffffffu, d, j);
+                    if (lane < n && j != lane && !(d == 0.0 && dj == 0.0) && fabs(dj - d) <= (d + dj) * 1e-13) rk = true;
+                }
+                if (__any_sync(0xffffffffu, rk) && lane == 0) risky = 1;
             }
-            if (__any_sync(0xffffffffu, rk) && lane == 0) risky = 1;
+        } else {
+            for (int i = n + t; i < p2; i += 128) {
+                cd[i] = DBL_MAX;
+                cid[i] = 0x7fffffff;
+            }
+            __syncthreads();
+            for (int size = 2; size <= p2; size <<= 1) {
+                for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                    for (int i = t; i < p2 / 2; i += 128) {
+                        int lo = 2 * i - (i & (stride - 1)), hi = lo + stride;
+                        bool up = (lo & size) == 0;
+                        double dl = cd[lo], dh = cd[hi];
+                        int il = cid[lo], ih = cid[hi];
+                        bool gt = (dl > dh) || (dl == dh && il > ih);
+                        if (gt == up) {
+                            cd[lo] = dh; cd[hi] = dl;
+                            cid[lo] = ih; cid[hi] = il;
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+            if (pass == 0)
+                for (int i = t; i + 1 < n; i += 128) {
+                    const double d = cd[i], dj = cd[i + 1];
+                    if (!(d == 0.0 && dj == 0.0) && dj - d <= (d + dj) * 1e-13) risky = 1;
+                }
         }
         __syncthreads();
-        if (!risky) break;
+        if (pass == 1 || !risky) break;
     }
     if (t == 0 && stats) atomicAdd(&stats[2], (unsigned long long)n);
     if (n <= 32) {
@@ -1174,29 +1220,7 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
         if (n < k && lane == 0) kth[q] = (float)infi_dis;
         return;
     }
-    int p2 = 1;
-    while (p2 < n) p2 <<= 1;
-    for (int i = n + t; i < p2; i += 128) {
-        cd[i] = DBL_MAX;
-        cid[i] = 0x7fffffff;
-    }
-    __syncthreads();
-    for (int size = 2; size <= p2; size <<= 1) {
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int i = t; i < p2 / 2; i += 128) {
-                int lo = 2 * i - (i & (stride - 1)), hi = lo + stride;
-                bool up = (lo & size) == 0;
-                double dl = cd[lo], dh = cd[hi];
-                int il = cid[lo], ih = cid[hi];
-                bool gt = (dl > dh) || (dl == dh && il > ih);
-                if (gt == up) {
-                    cd[lo] = dh; cd[hi] = dl;
-                    cid[lo] = ih; cid[hi] = il;
-                }
-            }
-            __syncthreads();
-        }
-    }
+    // sorted above
     if (t == 0) {
         int within = 0;
         for (int i = 0; i < n && i < k; i++) within += cd[i] * cd[i] <= lim;
@@ -1300,12 +1324,19 @@ static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
 
 static int launch_fast_tile(const FastTileArgs &a, int cg, int grid, cudaStream_t st)
 {
-    // k <= 8: the k kept bounds live in registers
+    // k <= 16: the k kept bounds live in registers
     if (a.k <= 8) {
         switch (cg) {
         case 4: return launch_fast_tile_cg<4, 8>(a, grid, st);
         case 2: return launch_fast_tile_cg<2, 8>(a, grid, st);
         default: return launch_fast_tile_cg<1, 8>(a, grid, st);
+        }
+    }
+    if (a.k <= 16) {
+        switch (cg) {
+        case 4: return launch_fast_tile_cg<4, 16>(a, grid, st);
+        case 2: return launch_fast_tile_cg<2, 16>(a, grid, st);
+        default: return launch_fast_tile_cg<1, 16>(a, grid, st);
         }
     }
     switch (cg) {
