@@ -243,11 +243,13 @@ __global__ void __launch_bounds__(256) k_fast_sbprep(int dim, const float *__res
 
 // One CTA per tile: the A operand of the tile's 128 queries (sorted by block
 // order), split into BF16 hi + lo, in the swizzled layout, and per lane
-// (query index, |q|^2, |q|).  A tile record is one bulk copy.
+// (query index, |q|^2, |q|).  A tile record is one bulk copy.  Beside it an
+// FP32 copy of the rows ([kp][128], zero padding) for the pruning kernels.
 __global__ void __launch_bounds__(128) k_fast_arec(const float *__restrict__ rows, const int *__restrict__ qids,
                                                    const int *__restrict__ order, int qnum, int dim, FastShape fs,
-                                                   unsigned char *__restrict__ arec)
+                                                   unsigned char *__restrict__ arec, float *__restrict__ qt)
 {
+    float *qtt = qt + (size_t)blockIdx.x * fs.kp * kFT;
     const int tile = blockIdx.x, lq = threadIdx.x;
     unsigned char *A_hi = arec + (size_t)tile * fs.arec_bytes, *A_lo = A_hi + fs.atile_bytes;
     int4 *info = reinterpret_cast<int4 *>(A_lo + fs.atile_bytes);
@@ -261,6 +263,7 @@ __global__ void __launch_bounds__(128) k_fast_arec(const float *__restrict__ row
         for (int u = 0; u < 8; u++) {
             int j = j0 + u;
             float x = (row && j < dim) ? row[j] : 0.f;
+            qtt[(size_t)j * kFT + lq] = x;
             acc += (double)x * x;
             hi[u] = f2bf(x);
             lo[u] = f2bf(x - bf2f(hi[u]));
@@ -343,9 +346,11 @@ struct NeedSmem {
     unsigned int flags[2];
 };
 
-__device__ __forceinline__ void need_load_tile(const float *__restrict__ rows, const int *__restrict__ qids,
-                               const unsigned char *__restrict__ arec, const FastShape &fs, int dim, int tile,
-                               const int *__restrict__ r2_bits, float *Qs, NeedSmem &sm)
+// The tile's query rows come from the FP32 copy k_fast_arec wrote in this
+// layout ([kp][128], zero padding): one contiguous 64 KB read.
+__device__ __forceinline__ void need_load_tile(const float *__restrict__ qt, const unsigned char *__restrict__ arec,
+                                               const FastShape &fs, int tile, const int *__restrict__ r2_bits,
+                                               float *Qs, NeedSmem &sm)
 {
     const int t = threadIdx.x;
     const int4 *info = reinterpret_cast<const int4 *>(arec + (size_t)tile * fs.arec_bytes + 2 * fs.atile_bytes);
@@ -355,29 +360,10 @@ __device__ __forceinline__ void need_load_tile(const float *__restrict__ rows, c
         sm.qns[t] = __int_as_float(in.z);
         sm.seeds[t] = in.x >= 0 ? __int_as_float(r2_bits[in.x]) : -1.f;
     }
-    // thread (l, h): query row l, every second group of 4 dimensions from h;
-    // shared-memory writes of a warp are consecutive queries (no conflicts)
-    const int l = t & (kFT - 1), h = t >> 7;
-    const int qi = info[l].x;
-    const float *row = qi >= 0 ? rows + (size_t)qids[qi] * dim : nullptr;
-    const bool vec = (dim & 3) == 0;
-    for (int j4 = h; j4 < fs.kp / 4; j4 += 2) {
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (row && 4 * j4 < dim) {
-            if (vec) {
-                v = *reinterpret_cast<const float4 *>(row + 4 * j4);
-            } else {
-                v.x = row[4 * j4];
-                v.y = 4 * j4 + 1 < dim ? row[4 * j4 + 1] : 0.f;
-                v.z = 4 * j4 + 2 < dim ? row[4 * j4 + 2] : 0.f;
-                v.w = 4 * j4 + 3 < dim ? row[4 * j4 + 3] : 0.f;
-            }
-        }
-        Qs[(4 * j4 + 0) * kFT + l] = v.x;
-        Qs[(4 * j4 + 1) * kFT + l] = v.y;
-        Qs[(4 * j4 + 2) * kFT + l] = v.z;
-        Qs[(4 * j4 + 3) * kFT + l] = v.w;
-    }
+    const float4 *src = reinterpret_cast<const float4 *>(qt + (size_t)tile * fs.kp * kFT);
+    float4 *dst = reinterpret_cast<float4 *>(Qs);
+#pragma unroll 4
+    for (int i = t; i < fs.kp * (kFT / 4); i += 256) dst[i] = src[i];
 }
 
 // Balls c0 .. c0+63 (those below cend; with a list, balls list[0 .. cend-1]
@@ -470,8 +456,8 @@ __device__ __forceinline__ uint64_t need_chunk(const float *__restrict__ cen, co
 
 // Superblocks the tile needs: CTA (tile, y) tests superblock chunk y and
 // writes its two mask words sb_mask[tile][2y .. 2y+1].
-__global__ void __launch_bounds__(256) k_need_sb(const float *__restrict__ rows, const int *__restrict__ qids,
-                                                 const unsigned char *__restrict__ arec, FastShape fs, int dim,
+__global__ void __launch_bounds__(256) k_need_sb(const float *__restrict__ qt,
+                                                 const unsigned char *__restrict__ arec, FastShape fs,
                                                  FastSummary bs, int nsb, const int *__restrict__ r2_bits,
                                                  uint32_t *__restrict__ sb_mask, int nsbw)
 {
@@ -479,7 +465,7 @@ __global__ void __launch_bounds__(256) k_need_sb(const float *__restrict__ rows,
     __shared__ NeedSmem sm;
     float *Qs = nsm, *Cs = nsm + fs.kp * kFT;
     const int tile = blockIdx.x, ch = blockIdx.y;
-    need_load_tile(rows, qids, arec, fs, dim, tile, r2_bits, Qs, sm);
+    need_load_tile(qt, arec, fs, tile, r2_bits, Qs, sm);
     const uint64_t m = need_chunk(bs.sb_cen, bs.sb_c2, bs.sb_rad, ch * kFChunk, nsb, nullptr, fs.kp, Qs, Cs, sm);
     if (threadIdx.x == 0) {
         sb_mask[(size_t)tile * nsbw + 2 * ch] = (uint32_t)m;
@@ -491,8 +477,8 @@ __global__ void __launch_bounds__(256) k_need_sb(const float *__restrict__ rows,
 // takes every gridDim.y-th needed superblock, gathers their blocks into
 // full chunks of kFChunk (superblocks hold 1..32 blocks) and appends the
 // needed ones to blist[tile][nbcap] (count in bcnt[tile]).
-__global__ void __launch_bounds__(256) k_need_blk(const float *__restrict__ rows, const int *__restrict__ qids,
-                                                  const unsigned char *__restrict__ arec, FastShape fs, int dim,
+__global__ void __launch_bounds__(256) k_need_blk(const float *__restrict__ qt,
+                                                  const unsigned char *__restrict__ arec, FastShape fs,
                                                   FastSummary bs, const int *__restrict__ r2_bits,
                                                   const uint32_t *__restrict__ sb_mask, int nsbw,
                                                   int *__restrict__ blist, int *__restrict__ bcnt, int nbcap,
@@ -513,7 +499,7 @@ __global__ void __launch_bounds__(256) k_need_blk(const float *__restrict__ rows
         seen += c;
     }
     if (mine == 0) return;
-    need_load_tile(rows, qids, arec, fs, dim, tile, r2_bits, Qs, sm);
+    need_load_tile(qt, arec, fs, tile, r2_bits, Qs, sm);
     unsigned long long tested = 0;
     int fill = 0, p = 0;
     int *dst = blist + (size_t)tile * nbcap;
@@ -1383,6 +1369,10 @@ static int fast_prepare(gts_index *idx, cudaStream_t st)
     idx->fast_recs = recs;
     idx->fast_nb = nb;
     idx->fast_nsb = nsb;
+    if (!idx->side_stream) {
+        GTS_CUDA_TRY(cudaStreamCreateWithFlags(&idx->side_stream, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; i++) GTS_CUDA_TRY(cudaEventCreateWithFlags(&idx->side_ev[i], cudaEventDisableTiming));
+    }
     idx->device_bytes += bytes;
     return GTS_OK;
 }
@@ -1391,6 +1381,7 @@ static int fast_prepare(gts_index *idx, cudaStream_t st)
 struct RunBufs {
     int *keys, *vals, *skeys, *order, *cpos, *ccnt, *r2, *ctr, *blist, *bcnt;
     float *clb, *cub_;
+    float *qt;   // [ntiles][kp][128] FP32 query rows of each tile
     unsigned char *arec;
     uint32_t *sb_mask;
     int2 *items;
@@ -1422,6 +1413,7 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
     r.ctr = (int *)take(8 * sizeof(int));   // failures, item counter, item count
     r.arec = take((size_t)ntiles * fs.arec_bytes);
     r.sb_mask = (uint32_t *)take(4 * (size_t)ntiles * std::max(nsbw, 1));
+    r.qt = (float *)take(4 * (size_t)ntiles * fs.kp * kFT);
     r.blist = (int *)take(4 * (size_t)ntiles * std::max(nb, 1));
     r.bcnt = (int *)take(4 * (size_t)ntiles);
     r.items = (int2 *)take(sizeof(int2) * std::max(itemcap, (size_t)1));
@@ -1457,29 +1449,45 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     int rc;
     const FastSummary bs = fast_summary(idx->fast_recs, fs, nb, nsb, idx->num);
 
-    k_fast_keys<<<(qnum + 255) / 256, 256, 0, st>>>(d_qids, qnum, bs.pos, r.keys, r.vals);
-    idx->kernel_launches++;
-    size_t cb = r.cub_bytes;
-    GTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(r.cub, cb, r.keys, r.skeys, r.vals, r.order, qnum, 0, 32, st));
     k_fast_init<<<(qnum + 255) / 256, 256, 0, st>>>(qnum, r.ccnt, r.r2, carry);
     idx->kernel_launches++;
     if (learned && (rc = mlp_seed(idx, d_qids, qnum, k, r.r2, st))) return rc;
+    // the certified own-block seed (with a learned radius the smaller of the
+    // two is used, and queries it under-predicts are answered again), on the
+    // side stream when the handle has one: it needs only the bounds, while
+    // the query sort and the tile operands proceed on st (inside a capture
+    // the two become parallel branches of the graph)
+    cudaStream_t ss = idx->side_stream ? idx->side_stream : st;
+    if (ss != st) {
+        GTS_CUDA_TRY(cudaEventRecord(idx->side_ev[0], st));
+        GTS_CUDA_TRY(cudaStreamWaitEvent(ss, idx->side_ev[0], 0));
+    }
+    k_fast_seed<<<qnum, 128, 0, ss>>>(idx->rows, d_qids, bs, idx->dim, fs.kp, k, r.r2);
+    idx->kernel_launches++;
+    k_fast_keys<<<(qnum + 255) / 256, 256, 0, st>>>(d_qids, qnum, bs.pos, r.keys, r.vals);
+    idx->kernel_launches++;
+    // slots are below nb * 128: sort only the bits they use
+    int key_bits = 1;
+    while (key_bits < 32 && (1ll << key_bits) < (long long)nb * kFB) key_bits++;
+    size_t cb = r.cub_bytes;
+    GTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(r.cub, cb, r.keys, r.skeys, r.vals, r.order, qnum, 0, key_bits,
+                                                 st));
     GTS_CUDA_TRY(cudaMemsetAsync(r.ctr, 0, 8 * sizeof(int), st));
     GTS_CUDA_TRY(cudaMemsetAsync(r.bcnt, 0, sizeof(int) * ntiles, st));
-    k_fast_arec<<<ntiles, 128, 0, st>>>(idx->rows, d_qids, r.order, qnum, idx->dim, fs, r.arec);
+    k_fast_arec<<<ntiles, 128, 0, st>>>(idx->rows, d_qids, r.order, qnum, idx->dim, fs, r.arec, r.qt);
     idx->kernel_launches++;
-    // the certified own-block seed; with a learned radius the smaller of the
-    // two is used, and queries it under-predicts are answered again
-    k_fast_seed<<<qnum, 128, 0, st>>>(idx->rows, d_qids, bs, idx->dim, fs.kp, k, r.r2);
-    idx->kernel_launches++;
+    if (ss != st) {
+        GTS_CUDA_TRY(cudaEventRecord(idx->side_ev[1], ss));
+        GTS_CUDA_TRY(cudaStreamWaitEvent(st, idx->side_ev[1], 0));
+    }
     const size_t need_smem = sizeof(float) * (size_t)fs.kp * (kFT + kFChunk);
     GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_sb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
     GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
     k_need_sb<<<dim3(ntiles, (nsb + kFChunk - 1) / kFChunk), 256, need_smem, st>>>(
-        idx->rows, d_qids, r.arec, fs, idx->dim, bs, nsb, r.r2, r.sb_mask, nsbw);
+        r.qt, r.arec, fs, bs, nsb, r.r2, r.sb_mask, nsbw);
     idx->kernel_launches++;
-    k_need_blk<<<dim3(ntiles, kNeedBlkY), 256, need_smem, st>>>(idx->rows, d_qids, r.arec, fs, idx->dim, bs, r.r2,
-                                                               r.sb_mask, nsbw, r.blist, r.bcnt, nb, idx->d_stats);
+    k_need_blk<<<dim3(ntiles, kNeedBlkY), 256, need_smem, st>>>(r.qt, r.arec, fs, bs, r.r2, r.sb_mask, nsbw,
+                                                               r.blist, r.bcnt, nb, idx->d_stats);
     idx->kernel_launches++;
     k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, r.bcnt, nb, cfg.item, r.items, r.ctr + 2);
     idx->kernel_launches++;

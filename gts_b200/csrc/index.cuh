@@ -62,6 +62,10 @@ struct gts_index {
     long long graph_launches = 0;
     long long graph_kernels = 0;   // this library's kernels in the captured graph
     bool graph_moved = false;      // the last capture was for moved argument buffers
+    // second stream of the filter pass: the own-block seeds run on it while
+    // the query sort and tile operands run on the first (fast.cu)
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t side_ev[2] = {nullptr, nullptr};
 
     // learned kNN radius (mlp.cu): parameters, input standardisation,
     // feature pivots; valid for the tree it was trained on
