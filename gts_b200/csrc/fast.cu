@@ -596,6 +596,7 @@ struct __align__(16) FastCtl {
     int blk[kFItemMax];    // the item's blocks
     int st_n;              // staged candidates (may run past st_cap: the rest went straight out)
     int st_cnt[kFT];       // staged candidates per query lane; at the flush: their list offset
+    int r2s[kFT];          // per query lane: the smallest bound its column groups reached (float bits)
 };
 
 // 12 bytes: the slot (< 2^25) with the query lane in the top 7 bits
@@ -694,7 +695,10 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
             ctl.nblk = nblk;
             ctl.st_n = 0;
         }
-        if (t < kFT) ctl.st_cnt[t] = 0;
+        if (t < kFT) {
+            ctl.st_cnt[t] = 0;
+            ctl.r2s[t] = __float_as_int(FLT_MAX);
+        }
         __syncthreads();
         const int tile = ctl.tile, nblk = ctl.nblk;
         if (tile < 0 || ctl.err) break;
@@ -790,6 +794,8 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                 }
                 tc_fence_after();
                 mbar_wait(&ctl.full[s], (uint32_t)((gi / kFS) & 1), kFWait);   // record tail visible here
+                // the bound the query's other column groups have reached
+                R2 = fminf(R2, __int_as_float(*(volatile const int *)&ctl.r2s[lq]));
                 const unsigned char *Bs = B0 + (size_t)s * rec_pad;
                 const float *tail = reinterpret_cast<const float *>(Bs + fs.btile_bytes);
                 const float *wv = tail + kTailW, *dn = tail + kTailDn;
@@ -921,6 +927,7 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                 // k distinct objects' upper bounds bound the query's k-th d^2
                 if (qi >= 0 && hmx < pub) {
                     atomicMin(a.r2_bits + qi, __float_as_int(fmaxf(hmx, 0.f)));
+                    if (CG > 1) atomicMin(&ctl.r2s[lq], __float_as_int(fmaxf(hmx, 0.f)));
                     pub = hmx;
                 }
                 tc_fence_before();
