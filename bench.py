@@ -10,7 +10,11 @@ One step = one batch of 10,000 queries through the search.  The data set
 (512 MB) is larger than the 126 MB L2, so no flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gts|reference]
-                    [--form fast|plain] [--k 8] [--queries 10000] [--n 1000000]
+                    [--form fast|plain|plain-learned] [--k 8 | --k-mix]
+                    [--queries 10000] [--n 1000000]
+
+--k-mix runs the same data with each query's k drawn uniformly from
+{1, 8, 32, 64}: one batch per k per step (the reference takes one k per run).
 
 --impl reference times the reference's own CUDA build (oracle/_ref, built
 from the reference sources) through its entry points on the same workload
@@ -124,10 +128,24 @@ def workload(args, rank=0):
     return rows, qids
 
 
+K_MIX = (1, 8, 32, 64)
+
+
+def k_groups(args, n_queries):
+    """(k, query positions) batches of one step.  --k-mix draws each query's k
+    uniformly from {1, 8, 32, 64} (seeded) and runs one batch per k, as the
+    reference takes one k per run; otherwise one batch with --k."""
+    if not args.k_mix:
+        return [(args.k, np.arange(n_queries))]
+    ks = np.random.default_rng(args.seed + 99).choice(np.array(K_MIX), size=n_queries)
+    return [(k, np.nonzero(ks == k)[0]) for k in K_MIX if (ks == k).any()]
+
+
 def config_dict(args, world):
-    return {"workload": f"gmm{args.n // 1000}k_d{args.dim}_l2_knn",
+    return {"workload": f"gmm{args.n // 1000}k_d{args.dim}_l2_knn" + ("_kmix" if args.k_mix else ""),
             "n": args.n, "dim": args.dim, "metric": "L2", "queries_per_gpu": args.queries,
-            "k": args.k, "tree_order": 10, "max_size": 20, "max_h": args.max_h,
+            "k": ("uniform over {1, 8, 32, 64}, one batch per k" if args.k_mix else args.k),
+            "tree_order": 10, "max_size": 20, "max_h": args.max_h,
             "form": args.form + ("" if args.form != "fast" else
                                  (" (block-pruned bf16 filter)" if args.no_learn else
                                   " (learned radius trained + block-pruned bf16 filter; " +
@@ -154,31 +172,35 @@ def run_reference(args):
         return 0
     from gts_b200 import datagen as G
     rows, qids = workload(args)
+    ref_kth = np.zeros(len(qids), np.float32)
+    t, wall, build_s = 0.0, 0.0, 0.0
     with tempfile.TemporaryDirectory() as tmp:
         dpath = os.path.join(tmp, "data.bin")
-        qpath = os.path.join(tmp, "q.txt")
         G.write_data_bin(dpath, 2, rows)
-        G.write_queries(qpath, qids)
-        out = os.path.join(tmp, "res.txt")
-        cmd = [drv, dpath, qpath, "0", str(args.k), out, "--order", "10", "--max-size", "20",
-               "--max-h", str(args.max_h), "--budget-gb", "6",
-               "--repeat", str(args.warmup + args.steps)]
-        t0 = time.time()
-        p = subprocess.run(cmd, capture_output=True, text=True, timeout=3000)
-        wall = time.time() - t0
-        lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
-        if p.returncode != 0 or not lines:
-            print(json.dumps({**base, "unavailable": f"reference run failed rc={p.returncode}: "
-                              f"{(p.stderr or p.stdout)[-300:]!r}"}))
-            return 0
-        info = json.loads(lines[-1])
-        runs = info["search_runs"][args.warmup:]
-        t = statistics.mean(runs)
+        # one reference run per k (it takes one k per run); a step is all of them
+        for k, sel in k_groups(args, len(qids)):
+            qpath = os.path.join(tmp, f"q{k}.txt")
+            G.write_queries(qpath, qids[sel])
+            out = os.path.join(tmp, f"res{k}.txt")
+            cmd = [drv, dpath, qpath, "0", str(k), out, "--order", "10", "--max-size", "20",
+                   "--max-h", str(args.max_h), "--budget-gb", "6",
+                   "--repeat", str(args.warmup + args.steps)]
+            t0 = time.time()
+            p = subprocess.run(cmd, capture_output=True, text=True, timeout=3000)
+            wall += time.time() - t0
+            lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+            if p.returncode != 0 or not lines:
+                print(json.dumps({**base, "unavailable": f"reference run failed rc={p.returncode}: "
+                                  f"{(p.stderr or p.stdout)[-300:]!r}"}))
+                return 0
+            info = json.loads(lines[-1])
+            t += statistics.mean(info["search_runs"][args.warmup:])
+            build_s += info["build_s"]
+            ref_kth[sel] = np.array([float(v) for v in open(out).read().split("\n")[2].split()], np.float32)
         value = args.queries / t
-        ref_kth = np.array([float(v) for v in open(out).read().split("\n")[2].split()], np.float32)
     line = {**base, "value": value, "ms_per_step": t * 1e3, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian mixture)",
-            "build_s": info["build_s"], "wall_s": wall,
+            "build_s": build_s, "wall_s": wall,
             "cpu_baseline": {"value": value, "unit": "queries/s", "cores": 1, "kind": "reference",
                              "sample": f"reference CUDA build (searchIndexKnnV2) on the B200, "
                                        f"{args.queries} queries per step, 6 GB list-table budget; "
@@ -192,20 +214,25 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ our arm
 
-def cpu_baseline(rows, qids, k, sample, kth_gpu):
-    """Exact multi-threaded brute force (reference leaf arithmetic) on the host."""
+def cpu_baseline(rows, qids, groups, sample, kth_gpu):
+    """Exact multi-threaded brute force (reference leaf arithmetic) on the host,
+    on the leading queries of each k batch (sample split evenly)."""
     from oracle import oracle as O
     ds = O.Dataset(2, rows)
-    q = qids[:sample]
     cores = os.cpu_count() or 1
-    t0 = time.perf_counter()
-    kth, _, _ = O.knn_brute(ds, q, k, nthreads=cores)
-    dt = time.perf_counter() - t0
-    agree = int((kth == kth_gpu[:sample]).sum())
-    return {"value": len(q) / dt, "unit": "queries/s", "cores": cores, "kind": "port",
-            "sample": f"{len(q)} of the {len(qids)} queries, exact brute force over all "
+    per = max(1, sample // len(groups))
+    n, agree, dt = 0, 0, 0.0
+    for g in groups:
+        sel = g["sel"][:per]
+        t0 = time.perf_counter()
+        kth, _, _ = O.knn_brute(ds, qids[sel], g["k"], nthreads=cores)
+        dt += time.perf_counter() - t0
+        agree += int((kth == kth_gpu[sel]).sum())
+        n += len(sel)
+    return {"value": n / dt, "unit": "queries/s", "cores": cores, "kind": "port",
+            "sample": f"{n} of the {len(qids)} queries, exact brute force over all "
                       f"{len(rows)} rows in the reference's F64 leaf arithmetic, {cores} threads",
-            "agrees_with_gpu": f"{agree}/{len(q)}"}
+            "agrees_with_gpu": f"{agree}/{n}"}
 
 
 def run_gts(args):
@@ -244,23 +271,39 @@ def run_gts(args):
         torch.cuda.synchronize()
         learn["train_s"] = time.perf_counter() - t0
         learn["n_train"] = args.train
-    Q, k = args.queries, args.k
-    d_q = torch.from_numpy(qids).to(dev)
-    d_kth = torch.empty(Q, dtype=torch.float32, device=dev)
+    Q = args.queries
+    # one batch per k (one in all unless --k-mix): device ids and results
+    groups = []
+    for k, sel in k_groups(args, Q):
+        groups.append({"k": k, "sel": sel, "q": torch.from_numpy(np.ascontiguousarray(qids[sel])).to(dev),
+                       "kth": torch.empty(len(sel), dtype=torch.float32, device=dev)})
+    k = groups[0]["k"] if len(groups) == 1 else None
+
+    def run_group(g):
+        idx.knn_device(g["q"].data_ptr(), len(g["sel"]), g["k"], g["kth"].data_ptr(), form=form,
+                       stream=stream.cuda_stream)
 
     def step():
-        idx.knn_device(d_q.data_ptr(), Q, k, d_kth.data_ptr(), form=form, stream=stream.cuda_stream)
+        for g in groups:
+            run_group(g)
 
     if learn is not None and args.form == "fast" and args.learned_seed != "auto":
-        step()   # tunes the configuration for k, then the seed choice is pinned
+        step()   # tunes the configuration for each k, then the seed choice is pinned
         torch.cuda.synchronize()
-        c = idx.fast_config(k)
-        idx.set_fast_config(k, args.learned_seed == "on", c["col_groups"], c["item_blocks"])
+        for g in groups:
+            c = idx.fast_config(g["k"])
+            idx.set_fast_config(g["k"], args.learned_seed == "on", c["col_groups"], c["item_blocks"])
     clocks = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    stats = idx.search_stats()
+    # work counters of one step (the library keeps those of its last call)
+    stats = {}
+    for g in groups:
+        run_group(g)
+        torch.cuda.synchronize()
+        for key, v in idx.search_stats().items():
+            stats[key] = stats.get(key, 0) + v
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -306,25 +349,31 @@ def run_gts(args):
         dist.barrier()
     ms_per_step = total_ms / args.steps
     value = world * Q * args.steps / (total_ms / 1e3)
-    kth_gpu = d_kth.cpu().numpy()
+    kth_gpu = np.zeros(Q, np.float32)
+    for g in groups:
+        kth_gpu[g["sel"]] = g["kth"].cpu().numpy()
 
     # end to end through the host-buffer API: H2D of the query ids from pinned
     # memory and D2H of the k-th distances inside every timed call
-    h_q = torch.from_numpy(qids).pin_memory().numpy()
+    for g in groups:
+        g["h_q"] = torch.from_numpy(np.ascontiguousarray(qids[g["sel"]])).pin_memory().numpy()
     for _ in range(max(1, args.warmup)):
-        idx.knn(h_q, k, form=form)
+        for g in groups:
+            idx.knn(g["h_q"], g["k"], form=form)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        kth_e2e = idx.knn(h_q, k, form=form)
+        kth_e2e = [idx.knn(g["h_q"], g["k"], form=form) for g in groups]
     e2e_s = time.perf_counter() - t0
     if world > 1:
         e2e_s = R.max_over_ranks(e2e_s, dist, dev)
     e2e = {"value": world * Q * args.steps / e2e_s, "unit": "queries/s",
-           "h2d_bytes_per_step": int(h_q.nbytes), "d2h_bytes_per_step": int(kth_e2e.nbytes)}
-    assert np.array_equal(kth_e2e, kth_gpu), "host-buffer and device-buffer paths disagree"
+           "h2d_bytes_per_step": int(sum(g["h_q"].nbytes for g in groups)),
+           "d2h_bytes_per_step": int(sum(x.nbytes for x in kth_e2e))}
+    for g, x in zip(groups, kth_e2e):
+        assert np.array_equal(x, kth_gpu[g["sel"]]), "host-buffer and device-buffer paths disagree"
 
     peaks = measured_peaks_all()
     d = args.dim
@@ -339,7 +388,8 @@ def run_gts(args):
             per_unit = json.load(f)
     if args.form != "fast":
         # every leaf row and pivot row a query reads, plus its own row and result
-        alg_bytes = 4 * d * (stats["objects"] + stats["pivots"]) + Q * (4 * d + 8 * k)
+        alg_bytes = 4 * d * (stats["objects"] + stats["pivots"]) + sum(len(g["sel"]) * (4 * d + 8 * g["k"])
+                                                                       for g in groups)
         achieved = alg_bytes / (launch_ms / 1e3) / 1e9
         traffic = None
         if "k_search" in per_unit:
@@ -384,12 +434,13 @@ def run_gts(args):
             "dtype": "f32/f64" if args.form != "fast" else "bf16/f32/f64",
             "data": "synthetic (seeded Gaussian mixture; the paper's data sets are absent)",
             "config": config_dict(args, world), "build_s": build_s, "learned_radius": learn,
-            "autotune": (idx.fast_config(k) if args.form == "fast"
-                         else {"threads_per_query_cta": idx.plain_threads(0)}),
+            "autotune": ((idx.fast_config(k) if k is not None else {str(g["k"]): idx.fast_config(g["k"])
+                                                                     for g in groups})
+                         if args.form == "fast" else {"threads_per_query_cta": idx.plain_threads(0)}),
             "roofline": roofline,
             "e2e": e2e, "gpu_launches": launches, "clocks": clock_summary}
     if rank == 0 and world == 1 and args.cpu_sample > 0:
-        line["cpu_baseline"] = cpu_baseline(rows, qids, k, args.cpu_sample, kth_gpu)
+        line["cpu_baseline"] = cpu_baseline(rows, qids, groups, args.cpu_sample, kth_gpu)
     if rank == 0:
         print(json.dumps(line))
     idx.close()
@@ -411,6 +462,8 @@ def main():
     ap.add_argument("--dim", type=int, default=128)
     ap.add_argument("--queries", type=int, default=10_000)
     ap.add_argument("--k", type=int, default=8)
+    ap.add_argument("--k-mix", action="store_true",
+                    help="k uniform over {1, 8, 32, 64} per query (one batch per k per step)")
     ap.add_argument("--max-h", type=int, default=6)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-sample", type=int, default=256)
