@@ -627,8 +627,8 @@ constexpr uint32_t kStagedUnused = 0xffffffffu;
 //
 // KH > 0 (k <= KH): each epilogue thread keeps its k smallest upper bounds in
 // registers (slots k..KH-1 hold -FLT_MAX and are never the largest); KH = 0:
-// as a binary max-heap
-// in shared memory, k per thread.
+// as a binary max-heap in shared memory, k per thread, each bound stored as
+// the upper 16 bits of its float rounded up (a bound again, 2 bytes).
 template <int CG, int KH>
 __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
 {
@@ -643,7 +643,7 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
     const uint32_t arec_pad = (fs.arec_bytes + 1023u) & ~1023u;
     const uint32_t rec_pad = (fs.rec_bytes + 1023u) & ~1023u;
     unsigned char *B0 = base + arec_pad;
-    float *heap = reinterpret_cast<float *>(B0 + kFS * rec_pad);
+    unsigned short *heap = reinterpret_cast<unsigned short *>(B0 + kFS * rec_pad);
     FastCtl &ctl = *reinterpret_cast<FastCtl *>(heap + (KH > 0 ? 0 : NT * a.k));
     FastStaged *stg = reinterpret_cast<FastStaged *>(&ctl + 1);
     const int st_cap = a.st_cap;
@@ -775,7 +775,7 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
 #pragma unroll
                 for (int h = 0; h < KH; h++) hreg[h] = h < k ? FLT_MAX : -FLT_MAX;
             } else {
-                for (int i = 0; i < k; i++) heap[i * NT + t] = FLT_MAX;
+                for (int i = 0; i < k; i++) heap[i * NT + t] = 0x7f80u;   // +inf
             }
             // the query's bound as published so far (its seed, tightened by
             // items of the same tile that finished earlier)
@@ -902,22 +902,26 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                                 // binary max-heap in shared memory: the root
                                 // (the largest kept bound) is replaced and
                                 // sifted down, log2(k) levels
+                                // (non-negative floats order like their
+                                // bit patterns)
+                                const uint32_t ubits = __float_as_uint(fmaxf(ub, 0.f));
+                                const unsigned short v = (unsigned short)((ubits + 0xffffu) >> 16);
                                 int i = 0;
                                 for (;;) {
                                     const int l = 2 * i + 1;
                                     if (l >= k) break;
-                                    float cv = heap[l * NT + t];
+                                    unsigned short cv = heap[l * NT + t];
                                     int c = l;
                                     if (l + 1 < k) {
-                                        const float rv = heap[(l + 1) * NT + t];
+                                        const unsigned short rv = heap[(l + 1) * NT + t];
                                         if (rv > cv) { cv = rv; c = l + 1; }
                                     }
-                                    if (cv <= ub) break;
+                                    if (cv <= v) break;
                                     heap[i * NT + t] = cv;
                                     i = c;
                                 }
-                                heap[i * NT + t] = ub;
-                                mx = heap[t];
+                                heap[i * NT + t] = v;
+                                mx = __uint_as_float((uint32_t)heap[t] << 16);
                             }
                             hmx = mx;
                             R2 = fminf(R2, mx);
@@ -1271,8 +1275,9 @@ __global__ void k_scatter_results(const int *idx, int n, int k, const float *kth
 // ---------------------------------------------------------------- host
 
 // Column groups per query lane: as many epilogue warps as the bound heaps
-// (threads x k floats, at most 32 KB of shared memory) allow.
-static int fast_cg(int k) { return k <= 16 ? 4 : (k <= 32 ? 2 : 1); }
+// (k <= 16 in registers; above, threads x k 2-byte entries, at most 32 KB of
+// shared memory) allow.
+static int fast_cg(int k) { return k <= 32 ? 4 : 2; }
 
 // One configuration of the fast form: seed with the learned radius or not,
 // epilogue column groups (warps per query lane), blocks per work item.
@@ -1296,7 +1301,7 @@ static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
 {
     const uint32_t arec_pad = (a.fs.arec_bytes + 1023u) & ~1023u;
     const uint32_t rec_pad = (a.fs.rec_bytes + 1023u) & ~1023u;
-    const size_t heap = KH > 0 ? 0 : sizeof(float) * 128 * CG * (size_t)a.k;
+    const size_t heap = KH > 0 ? 0 : sizeof(unsigned short) * 128 * CG * (size_t)a.k;
     const size_t fixed = 1024 + (size_t)arec_pad + kFS * (size_t)rec_pad + heap + sizeof(FastCtl) + 64;
     int dev = 0, optin = 0;
     GTS_CUDA_TRY(cudaGetDevice(&dev));
@@ -1785,7 +1790,7 @@ static int fast_autotune(gts_index *idx, FastCall &fc, int qc, const int *d_qids
     int rc = GTS_OK;
     for (int learned = 0; learned <= (idx->mlp_ready ? 1 : 0) && rc == GTS_OK; learned++)
         for (int cg = 4; cg >= 1 && rc == GTS_OK; cg >>= 1) {
-            if (cg * k > 64) continue;   // heaps: 128 cg threads x k floats <= 32 KB
+            if (k > 16 && cg * k > 128) continue;   // heaps: 128 cg threads x k x 2 bytes <= 32 KB
             for (int item = 8; item <= kFItemMax && rc == GTS_OK; item *= 2) {
                 const FastCfg c{learned != 0, cg, item};
                 if ((rc = (int)cudaEventRecord(e0, st)) != 0) {
@@ -1918,8 +1923,8 @@ extern "C" int gts_fast_config(const gts_index *idx, int k, int *tuned, int *lea
 extern "C" int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int item_blocks)
 {
     if (!idx || k < 1 || k > gts::kFMaxK || (col_groups != 1 && col_groups != 2 && col_groups != 4) ||
-        col_groups * k > 64 || (item_blocks != 8 && item_blocks != 16 && item_blocks != 32)) {
-        gts_set_error("gts_fast_config_set: k in [1, 64], column groups 1/2/4 with groups * k <= 64, "
+        col_groups * k > 128 || (item_blocks != 8 && item_blocks != 16 && item_blocks != 32)) {
+        gts_set_error("gts_fast_config_set: k in [1, 64], column groups 1/2/4 with groups * k <= 128, "
                       "8/16/32 blocks per item");
         return GTS_ERR_INVALID;
     }

@@ -145,7 +145,7 @@ int gts_kernel_launches(const gts_index *idx, long long *count);
 int gts_fast_config(const gts_index *idx, int k, int *tuned, int *learned, int *col_groups, int *item_blocks);
 
 /* Pin the configuration for k (learned seed 0/1, 1/2/4 column groups with
- * groups * k <= 64, 8/16/32 blocks per item) instead of tuning it. */
+ * groups * k <= 128, 8/16/32 blocks per item) instead of tuning it. */
 int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int item_blocks);
 
 /* Forget the tuned configurations (the next large batch tunes again). */
