@@ -1498,7 +1498,10 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     k_need_sb<<<dim3(ntiles, (nsb + kFChunk - 1) / kFChunk), 256, need_smem, st>>>(
         r.qt, r.arec, fs, bs, nsb, r.r2, r.sb_mask, nsbw);
     idx->kernel_launches++;
-    k_need_blk<<<dim3(ntiles, kNeedBlkY), 256, need_smem, st>>>(r.qt, r.arec, fs, bs, r.r2, r.sb_mask, nsbw,
+    // CTAs per tile: at least kNeedBlkY, more for small batches so that
+    // about four CTAs per SM share the needed superblocks
+    const int need_y = std::max(kNeedBlkY, std::min(32, (4 * nsm + ntiles - 1) / ntiles));
+    k_need_blk<<<dim3(ntiles, need_y), 256, need_smem, st>>>(r.qt, r.arec, fs, bs, r.r2, r.sb_mask, nsbw,
                                                                r.blist, r.bcnt, nb, idx->d_stats);
     idx->kernel_launches++;
     k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, r.bcnt, nb, cfg.item, r.items, r.ctr + 2);
