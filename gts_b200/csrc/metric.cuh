@@ -176,24 +176,6 @@ __device__ __forceinline__ float warp_max(float v)
     return v;
 }
 
-// dist_row_f64 for L2, with the terms spread over a warp: lane j % 32
-// evaluates pow(a[j] - b[j], 2) into buf[j] (dim doubles of shared memory
-// owned by the warp) and lane 0 adds them in j order, so the value is the
-// sequential one bit for bit.  Every lane receives the result.
-__device__ __forceinline__ double warp_dist_l2_f64(const float *__restrict__ a, const float *__restrict__ b,
-                                                   int dim, int lane, double *buf)
-{
-    for (int j = lane; j < dim; j += 32) buf[j] = pow(a[j] - b[j], 2);
-    __syncwarp();
-    double r = 0.0;
-    if (lane == 0) {
-        for (int j = 0; j < dim; j++) r += buf[j];
-        r = pow(r, 0.5);
-    }
-    __syncwarp();
-    return __shfl_sync(0xffffffffu, r, 0);
-}
-
 // Relative bound on |fp32 sum of n non-negative terms - exact sum| / sum,
 // terms themselves rounded once: (n + 2) u / (1 - (n + 2) u), u = 2^-24.
 __host__ __device__ __forceinline__ float f32_sum_rel_bound(int n)
