@@ -325,15 +325,25 @@ class Index:
                                         C.c_void_p(d_kth), C.c_void_p(d_ids or None),
                                         C.c_void_p(d_dists or None), C.c_void_p(stream)))
 
-    def range(self, qids, r: float) -> np.ndarray:
+    def range(self, qids, r: float, form: int = FORM_PLAIN) -> np.ndarray:
+        """Count of objects within r of each query (itself included);
+        form=FORM_FAST runs the tensor-core filter (L2, dim <= 128)."""
         q = np.ascontiguousarray(qids, dtype=np.int32)
         out = np.empty(len(q), np.int32)
-        _check(self._lib.gts_range(self._h, _ip(q), len(q), C.c_float(r), _ip(out)))
+        if form == FORM_PLAIN:
+            _check(self._lib.gts_range(self._h, _ip(q), len(q), C.c_float(r), _ip(out)))
+        else:
+            _check(self._lib.gts_range_form(self._h, _ip(q), len(q), C.c_float(r), int(form), _ip(out)))
         return out
 
-    def range_device(self, d_qids: int, qnum: int, r: float, d_counts: int, stream: int = 0):
-        _check(self._lib.gts_range_device(self._h, C.c_void_p(d_qids), qnum, C.c_float(r),
-                                          C.c_void_p(d_counts), C.c_void_p(stream)))
+    def range_device(self, d_qids: int, qnum: int, r: float, d_counts: int, stream: int = 0,
+                     form: int = FORM_PLAIN):
+        if form == FORM_PLAIN:
+            _check(self._lib.gts_range_device(self._h, C.c_void_p(d_qids), qnum, C.c_float(r),
+                                              C.c_void_p(d_counts), C.c_void_p(stream)))
+        else:
+            _check(self._lib.gts_range_form_device(self._h, C.c_void_p(d_qids), qnum, C.c_float(r), int(form),
+                                                   C.c_void_p(d_counts), C.c_void_p(stream)))
 
     def range_ids(self, qids, r: float, capacity: int | None = None):
         """-> (counts, offsets, ids, dists); each query's hits in (distance, id) order."""

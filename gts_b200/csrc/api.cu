@@ -569,6 +569,43 @@ extern "C" int gts_range(gts_index *idx, const int *qids, int qnum, float r, int
     return GTS_OK;
 }
 
+extern "C" int gts_range_form_device(gts_index *idx, const int *d_qids, int qnum, float r, int form,
+                                     int *d_counts, void *stream)
+{
+    if (!idx || qnum < 0 || (qnum > 0 && (!d_qids || !d_counts)) ||
+        (form != GTS_FORM_PLAIN && form != GTS_FORM_FAST)) {
+        gts_set_error("gts_range_form_device: invalid argument (form must be GTS_FORM_PLAIN or GTS_FORM_FAST)");
+        return GTS_ERR_INVALID;
+    }
+    if (form == GTS_FORM_FAST) return gts::search_range_fast(idx, d_qids, qnum, r, d_counts, (cudaStream_t)stream);
+    return gts::search_range(idx, d_qids, qnum, r, d_counts, nullptr, (cudaStream_t)stream);
+}
+
+extern "C" int gts_range_form(gts_index *idx, const int *qids, int qnum, float r, int form, int *counts_out)
+{
+    if (!idx || qnum < 0 || (qnum > 0 && (!qids || !counts_out)) ||
+        (form != GTS_FORM_PLAIN && form != GTS_FORM_FAST)) {
+        gts_set_error("gts_range_form: invalid argument (form must be GTS_FORM_PLAIN or GTS_FORM_FAST)");
+        return GTS_ERR_INVALID;
+    }
+    if (qnum == 0) return GTS_OK;
+    int rc = check_qids(idx, qids, qnum);
+    if (rc) return rc;
+    cudaStream_t s = idx->stream;
+    IoCarve io;
+    io.add(sizeof(int) * (size_t)qnum);
+    io.add(sizeof(int) * (size_t)qnum);
+    void *buf[2];
+    if ((rc = io.get(idx, buf))) return rc;
+    GTS_CUDA_TRY(cudaMemcpyAsync(buf[0], qids, sizeof(int) * (size_t)qnum, cudaMemcpyHostToDevice, s));
+    rc = form == GTS_FORM_FAST ? gts::search_range_fast(idx, (int *)buf[0], qnum, r, (int *)buf[1], s)
+                               : gts::search_range(idx, (int *)buf[0], qnum, r, (int *)buf[1], nullptr, s);
+    if (rc) return rc;
+    GTS_CUDA_TRY(cudaMemcpyAsync(counts_out, buf[1], sizeof(int) * (size_t)qnum, cudaMemcpyDeviceToHost, s));
+    GTS_CUDA_TRY(cudaStreamSynchronize(s));
+    return GTS_OK;
+}
+
 extern "C" int gts_range_ids(gts_index *idx, const int *qids, int qnum, float r, int *counts_out,
                              int *offsets_out, int *ids_out, float *dists_out, size_t capacity)
 {

@@ -44,7 +44,9 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <algorithm>
 #include <cfloat>
+#include <cmath>
 #include <cstdio>
+#include <cstring>
 #include "fast.cuh"
 #include "sm100.cuh"
 
@@ -576,6 +578,10 @@ struct FastTileArgs {
     int *item_counter;           // persistent-CTA work queue
     int *status;
     unsigned long long *stats;
+    // range counts (k_fast_tile<.., true>): objects whose upper bound is
+    // below r2lo are counted in rcnt[query] without a list entry
+    float r2lo;
+    int *rcnt;
 };
 
 constexpr int kFS = 3;         // block stages, each with its own TMEM accumulator
@@ -629,7 +635,11 @@ constexpr uint32_t kStagedUnused = 0xffffffffu;
 // registers (slots k..KH-1 hold -FLT_MAX and are never the largest); KH = 0:
 // as a binary max-heap in shared memory, k per thread, each bound stored as
 // the upper 16 bits of its float rounded up (a bound again, 2 bytes).
-template <int CG, int KH>
+//
+// RANGE: range counts instead of kNN.  The bound stays the query's (r^2 with
+// the reference-arithmetic margin); objects certainly inside are counted per
+// thread, only the uncertain ones are listed; no bound heap.
+template <int CG, int KH, bool RANGE>
 __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
 {
     constexpr int NT = 128 * CG;   // epilogue threads
@@ -782,6 +792,7 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
             const float seed = qi >= 0 ? __int_as_float(*(volatile const int *)(a.r2_bits + qi)) : FLT_MAX;
             float R2 = seed, pub = seed;   // bound in use, last bound published
             float hmx = FLT_MAX;           // largest of this thread's k kept upper bounds
+            int certain = 0;               // range: objects certainly within r
             int hidx = 0;
             const uint32_t trow = (uint32_t)(warp & 3) * 32u << 16;
             for (int j = 0; j < nblk; j++) {
@@ -829,8 +840,10 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                     __syncwarp();   // tcgen05.ld is warp-collective: reconverge after the appends
                     tmem_ld16_nowait(taddr + (uint32_t)c, r);
                     tmem_wait_ld(r);
-                    uint32_t pass = 0;
+                    uint32_t pass = 0, inside = 0;
                     const float RT = R2 - T;
+                    // range: ub < r2lo, with the comparison's own rounding covered
+                    const float RLT = a.r2lo - T - 2e-6f * q2;
 #pragma unroll
                     for (int u4 = 0; u4 < 4; u4++) {
                         const float4 w4 = *reinterpret_cast<const float4 *>(wv + c + 4 * u4);
@@ -842,9 +855,14 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                             // lb - T; padding objects have w = +inf and never pass
                             const float x = fmaf(-2.f, __uint_as_float(r[u]), fmaf(-A, dq[e], wq[e]));
                             pass |= (x <= RT ? 1u : 0u) << u;
+                            if constexpr (RANGE) inside |= (x + 2.f * fmaf(A, dq[e], eb) < RLT ? 1u : 0u) << u;
                         }
                     }
-                    if (skip) pass = 0;
+                    if (skip) pass = inside = 0;
+                    if constexpr (RANGE) {
+                        pass &= ~inside;
+                        certain += __popc(inside);
+                    }
                     // staging: one shared-memory reservation per warp (prefix
                     // sum of the lanes' counts), one rank reservation per lane
                     if (!__any_sync(0xffffffffu, pass != 0)) continue;
@@ -888,7 +906,7 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                             }
                             gsl++;
                         }
-                        if (ub < R2) {   // replace the largest of the k kept bounds
+                        if (!RANGE && ub < R2) {   // replace the largest of the k kept bounds
                             float mx = -FLT_MAX;
                             if constexpr (KH > 0) {
                                 int mi = 0;
@@ -929,7 +947,7 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                     }
                 }
                 // k distinct objects' upper bounds bound the query's k-th d^2
-                if (qi >= 0 && hmx < pub) {
+                if (!RANGE && qi >= 0 && hmx < pub) {
                     atomicMin(a.r2_bits + qi, __float_as_int(fmaxf(hmx, 0.f)));
                     if (CG > 1) atomicMin(&ctl.r2s[lq], __float_as_int(fmaxf(hmx, 0.f)));
                     pub = hmx;
@@ -938,6 +956,7 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&ctl.efree[s]);
             }
+            if (RANGE && qi >= 0 && certain) atomicAdd(a.rcnt + qi, certain);
         }
         gblk += nblk;
         tc_fence_before();
@@ -1253,6 +1272,12 @@ __global__ void k_fast_init(int qnum, int *cand_cnt, int *r2_bits, const int *ca
 
 __global__ void k_add_stat(unsigned long long *p, unsigned long long v) { *p += v; }
 
+__global__ void k_scatter_i(const int *idx, int n, const int *src, int *dst)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[idx[i]] = src[i];
+}
+
 __global__ void k_gather_i(const int *src, const int *idx, int n, int *dst)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1296,7 +1321,7 @@ static FastCfg fast_default_cfg(const gts_index *idx, int k)
     return FastCfg{idx->mlp_ready && k >= 16, fast_cg(k), 16};
 }
 
-template <int CG, int KH>
+template <int CG, int KH, bool RANGE = false>
 static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
 {
     const uint32_t arec_pad = (a.fs.arec_bytes + 1023u) & ~1023u;
@@ -1314,8 +1339,9 @@ static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
         return GTS_ERR_INVALID;
     }
     const size_t smem = fixed + sizeof(FastStaged) * (size_t)b.st_cap;
-    GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_tile<CG, KH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_fast_tile<CG, KH><<<grid, 128 * CG + 32, smem, st>>>(b);
+    GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_tile<CG, KH, RANGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    k_fast_tile<CG, KH, RANGE><<<grid, 128 * CG + 32, smem, st>>>(b);
     GTS_CUDA_TRY(cudaGetLastError());
     return GTS_OK;
 }
@@ -1527,6 +1553,8 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     a.item_counter = r.ctr + 1;
     a.status = idx->d_status;
     a.stats = idx->d_stats;
+    a.r2lo = 0.f;
+    a.rcnt = nullptr;
     // events inside a captured graph must be external records to time it
     if (timed)
         GTS_CUDA_TRY(cudaEventRecordWithFlags(idx->fev[0], st, capturing ? cudaEventRecordExternal : 0));
@@ -1893,6 +1921,170 @@ int search_knn_fast_fixed(gts_index *idx, const int *d_qids, int qnum, int k, fl
                                                            d_ids, d_dists);
     idx->kernel_launches++;
     GTS_CUDA_TRY(cudaGetLastError());
+    GTS_CUDA_TRY(cudaStreamSynchronize(st));
+    return GTS_OK;
+}
+
+// ---------------------------------------------------------------- range counts
+
+__global__ void k_fast_range_init(int qnum, int *cand_cnt, int *r2_bits, int *rcnt, int r2hi_bits)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < qnum) {
+        cand_cnt[i] = 0;
+        r2_bits[i] = r2hi_bits;
+        rcnt[i] = 0;
+    }
+}
+
+// One CTA per query: the listed (uncertain) objects get the reference's
+// range value (searchIndexRnnV2's leaf: FP32 accumulation of pow terms, then
+// pow(., 0.5); the query itself at 0) and count when it is within r; the
+// count adds to the objects the filter found certainly inside.  A query
+// whose list overflowed goes to the overflow list.
+__global__ void __launch_bounds__(128) k_fast_range_final(const float *__restrict__ rows, int dim, int num,
+                                                          const float *__restrict__ prow, int kp,
+                                                          const int *__restrict__ ids_of_slot, int nslots,
+                                                          const int *__restrict__ qids, float r,
+                                                          const int *__restrict__ cand_pos,
+                                                          const int *__restrict__ cand_cnt,
+                                                          const int *__restrict__ rcnt, int *counts, int *overflow,
+                                                          int *n_overflow, unsigned long long *stats)
+{
+    __shared__ int c;
+    const int q = blockIdx.x, t = threadIdx.x;
+    const int cnt = cand_cnt[q];
+    if (cnt > kFCand) {
+        if (t == 0) overflow[atomicAdd(n_overflow, 1)] = q;
+        return;
+    }
+    if (t == 0) c = 0;
+    __syncthreads();
+    const int qid = qids[q];
+    const float *qrow = rows + (size_t)qid * dim;
+    for (int i = t; i < cnt; i += 128) {
+        const int slot = cand_pos[(size_t)q * kFCand + i];
+        if (slot < 0 || slot >= nslots) continue;
+        const int id = ids_of_slot[slot];
+        if (id < 0 || id >= num) continue;
+        const float d = id == qid ? 0.f : dist_row_f32(prow + (size_t)slot * kp, qrow, dim, kL2);
+        if (d <= r) atomicAdd(&c, 1);
+    }
+    __syncthreads();
+    if (t == 0) {
+        counts[q] = rcnt[q] + c;
+        if (stats) atomicAdd(&stats[2], (unsigned long long)cnt);
+    }
+}
+
+// Range counts on the tensor cores (L2, dim <= 128): the fast form's block
+// order, pruning and filter with the bound fixed at r^2.  The reference's
+// value is an FP32 accumulation (relative error below (dim + 2) 2^-24 on the
+// square, under 8e-6 at dim 128), so an object whose certified upper bound
+// on d^2 is below r^2 (1 - 3e-5) is within r in the reference's arithmetic
+// too and is counted directly; one whose lower bound is above r^2 (1 + 3e-5)
+// is not; the rest get the reference's value.  Queries whose list of
+// uncertain objects overflowed are counted by the plain traversal.
+int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int *d_counts, cudaStream_t st)
+{
+    if (!fast_supported(idx, 1) || !(r >= 0.f)) return search_range(idx, d_qids, qnum, r, d_counts, nullptr, st);
+    if (qnum <= 0) return GTS_OK;
+    int rc = fast_prepare(idx, st);
+    if (rc) return rc;
+    const FastShape fs = fast_shape(idx->dim);
+    const int nb = idx->fast_nb, nsb = idx->fast_nsb, nsbw = (nsb + 31) / 32;
+    const int qc = std::min(qnum, kFMaxBatch);
+    const size_t rbytes = (plan_run(idx, qc, nullptr, nullptr) + 255) & ~(size_t)255;
+    const size_t ib = ((size_t)qc * sizeof(int) + 255) & ~(size_t)255;
+    if ((rc = ensure_scratch(idx, rbytes + 4 * ib))) return rc;
+    unsigned char *region = (unsigned char *)idx->scratch;
+    int *rcnt = (int *)(region + rbytes), *fail = (int *)(region + rbytes + ib);
+    int *sub_q = (int *)(region + rbytes + 2 * ib), *sub_c = (int *)(region + rbytes + 3 * ib);
+    const double rr = (double)r * (double)r;
+    // r^2 (1 + 3e-5) rounded up and r^2 (1 - 3e-5) rounded down to float
+    float r2hi = (float)(rr * (1.0 + 3e-5)), r2lo = (float)(rr * (1.0 - 3e-5));
+    if ((double)r2hi < rr * (1.0 + 3e-5)) r2hi = std::nextafter(r2hi, INFINITY);
+    if ((double)r2lo > rr * (1.0 - 3e-5)) r2lo = std::nextafter(r2lo, 0.f);
+    int r2hi_bits;
+    std::memcpy(&r2hi_bits, &r2hi, sizeof(int));
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const FastSummary bs = fast_summary(idx->fast_recs, fs, nb, nsb, idx->num);
+    GTS_CUDA_TRY(cudaMemsetAsync(idx->d_status, 0, sizeof(int), st));
+    if (!idx->keep_stats) GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, kStatsN * sizeof(unsigned long long), st));
+    int key_bits = 1;
+    while (key_bits < 32 && (1ll << key_bits) < (long long)nb * kFB) key_bits++;
+    for (int q0 = 0; q0 < qnum; q0 += qc) {
+        const int n = std::min(qc, qnum - q0);
+        const int *dq = d_qids + q0;
+        const int ntiles = (n + kFT - 1) / kFT;
+        RunBufs rb;
+        plan_run(idx, n, region, &rb);
+        k_fast_keys<<<(n + 255) / 256, 256, 0, st>>>(dq, n, bs.pos, rb.keys, rb.vals);
+        size_t cb = rb.cub_bytes;
+        GTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(rb.cub, cb, rb.keys, rb.skeys, rb.vals, rb.order, n, 0,
+                                                     key_bits, st));
+        k_fast_range_init<<<(n + 255) / 256, 256, 0, st>>>(n, rb.ccnt, rb.r2, rcnt, r2hi_bits);
+        GTS_CUDA_TRY(cudaMemsetAsync(rb.ctr, 0, 8 * sizeof(int), st));
+        GTS_CUDA_TRY(cudaMemsetAsync(rb.bcnt, 0, sizeof(int) * ntiles, st));
+        k_fast_arec<<<ntiles, 128, 0, st>>>(idx->rows, dq, rb.order, n, idx->dim, fs, rb.arec, rb.qt);
+        const size_t need_smem = sizeof(float) * (size_t)fs.kp * (kFT + kFChunk);
+        GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_sb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
+        GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
+        k_need_sb<<<dim3(ntiles, (nsb + kFChunk - 1) / kFChunk), 256, need_smem, st>>>(
+            rb.qt, rb.arec, fs, bs, nsb, rb.r2, rb.sb_mask, nsbw);
+        const int need_y = std::max(kNeedBlkY, std::min(32, (4 * nsm + ntiles - 1) / ntiles));
+        k_need_blk<<<dim3(ntiles, need_y), 256, need_smem, st>>>(rb.qt, rb.arec, fs, bs, rb.r2, rb.sb_mask, nsbw,
+                                                                 rb.blist, rb.bcnt, nb, idx->d_stats);
+        k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, rb.bcnt, nb, 16, rb.items, rb.ctr + 2);
+        GTS_CUDA_TRY(cudaGetLastError());
+        FastTileArgs a;
+        a.recs = idx->fast_recs;
+        a.arec = rb.arec;
+        a.blist = rb.blist;
+        a.bcnt = rb.bcnt;
+        a.items = rb.items;
+        a.n_items = rb.ctr + 2;
+        a.nbcap = nb;
+        a.k = 1;
+        a.item = 16;
+        a.fs = fs;
+        a.cand_pos = rb.cpos;
+        a.cand_lb = rb.clb;
+        a.cand_ub = rb.cub_;
+        a.cand_cnt = rb.ccnt;
+        a.r2_bits = rb.r2;
+        a.item_counter = rb.ctr + 1;
+        a.status = idx->d_status;
+        a.stats = idx->d_stats;
+        a.r2lo = r2lo;
+        a.rcnt = rcnt;
+        if ((rc = launch_fast_tile_cg<4, 8, true>(a, nsm, st))) return rc;
+        k_fast_range_final<<<n, 128, 0, st>>>(idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, dq, r,
+                                              rb.cpos, rb.ccnt, rcnt, d_counts + q0, fail, rb.ctr, idx->d_stats);
+        idx->kernel_launches += 10;
+        GTS_CUDA_TRY(cudaGetLastError());
+        int status = 0, n_fail = 0;
+        GTS_CUDA_TRY(cudaMemcpyAsync(&status, idx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+        GTS_CUDA_TRY(cudaMemcpyAsync(&n_fail, rb.ctr, sizeof(int), cudaMemcpyDeviceToHost, st));
+        GTS_CUDA_TRY(cudaStreamSynchronize(st));
+        if (status != 0) {
+            gts_set_error("tensor-core filter kernel reported status %d (barrier wait gave up)", status);
+            return GTS_ERR_KERNEL;
+        }
+        if (n_fail > 0) {
+            // overflowed lists: the plain traversal counts those queries
+            k_gather_i<<<(n_fail + 255) / 256, 256, 0, st>>>(dq, fail, n_fail, sub_q);
+            idx->keep_stats = true;
+            rc = search_range(idx, sub_q, n_fail, r, sub_c, nullptr, st);
+            idx->keep_stats = false;
+            if (rc) return rc;
+            k_scatter_i<<<(n_fail + 255) / 256, 256, 0, st>>>(fail, n_fail, sub_c, d_counts + q0);
+            idx->kernel_launches += 2;
+            GTS_CUDA_TRY(cudaGetLastError());
+        }
+    }
     GTS_CUDA_TRY(cudaStreamSynchronize(st));
     return GTS_OK;
 }

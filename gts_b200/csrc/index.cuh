@@ -99,6 +99,7 @@ int search_knn(gts_index *idx, const int *d_qids, int qnum, int k, int form,
                float *d_kth, int *d_ids, float *d_dists, cudaStream_t s);
 int search_range(gts_index *idx, const int *d_qids, int qnum, float r, int *d_counts,
                  const uint32_t *d_deleted, cudaStream_t s);
+int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int *d_counts, cudaStream_t s);
 int search_range_ids(gts_index *idx, const int *d_qids, int qnum, float r, int *d_counts,
                      int *d_ids, float *d_dists, const int *d_offsets, cudaStream_t s);
 

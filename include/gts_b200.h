@@ -205,6 +205,18 @@ int gts_range(gts_index *idx, const int *qids, int qnum, float r, int *counts_ou
 int gts_range_device(gts_index *idx, const int *d_qids, int qnum, float r,
                      int *d_counts, void *stream);
 
+/* searchIndexRnnV2 (search_v2.cuh:780-972) -> res, as gts_range, in a
+ * chosen form.  GTS_FORM_FAST (L2, dim <= 128; other indexes take the plain
+ * form): the tensor-core filter with the bound fixed at r^2; objects whose
+ * certified upper bound lies below r^2 (1 - 3e-5) count without a recheck
+ * (the reference's FP32-accumulated value is within 8e-6 of the square),
+ * those whose lower bound lies above r^2 (1 + 3e-5) do not, and the rest get
+ * the reference's value.  The counts equal gts_range's. */
+int gts_range_form(gts_index *idx, const int *qids, int qnum, float r, int form, int *counts_out);
+
+int gts_range_form_device(gts_index *idx, const int *d_qids, int qnum, float r, int form,
+                          int *d_counts, void *stream);
+
 /* saveR layout (file.cuh:178-199): ids of every object within r.
  * counts_out[q] as above, offsets_out[q] = exclusive prefix of counts,
  * ids_out/dists_out hold up to `capacity` entries grouped by query in

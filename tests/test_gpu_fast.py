@@ -126,3 +126,35 @@ def test_fast_exact_ties_from_duplicate_rows(oracle):
             np.testing.assert_array_equal(ids, bi, err_msg=f"k={k}")
             np.testing.assert_array_equal(kth, bk, err_msg=f"k={k}")
             np.testing.assert_array_equal(dis, bd, err_msg=f"k={k}")
+
+
+@pytest.mark.parametrize("n,dim,comps,sigma,max_h", [(20000, 128, 32, 0.2, 5), (7777, 100, 8, 0.25, 4)])
+def test_fast_range_counts_equal_brute_force(oracle, n, dim, comps, sigma, max_h):
+    """Range counts through the tensor-core filter equal exact brute force in
+    the reference's range arithmetic and the plain traversal's counts, from
+    radius 0 (the query itself) to radii holding thousands of objects."""
+    rows = G.gmm_rows(n, dim, comps, sigma, seed=n + 7)
+    ds = oracle.Dataset(2, rows)
+    q = G.query_ids(n, 300, seed=n + 8)
+    with gts.Index(rows, 2, max_h=max_h) as idx:
+        for frac in (0.0, 0.001, 0.01, 0.2):
+            r = 0.0 if frac == 0 else float(np.float32(G.quantile_radius(2, frac, 20000, n + 9, rows=rows)))
+            fast = idx.range(q, r, form=gts.FORM_FAST)
+            np.testing.assert_array_equal(fast, oracle.range_brute(ds, q, r), err_msg=f"r={r}")
+            np.testing.assert_array_equal(fast, idx.range(q, r), err_msg=f"r={r}")
+
+
+def test_fast_range_overflow_goes_to_the_plain_traversal(oracle):
+    """1,500 copies of one row just inside the radius (1e-6 relative, well
+    beyond rounding, well inside the filter's 3e-5 band): every copy is
+    uncertain to the filter, the query's list overflows and the plain
+    traversal counts it."""
+    base = G.gmm_rows(5000, 64, 8, 0.3, seed=71)
+    rows = np.concatenate([base, np.repeat(base[7:8], 1500, axis=0)])
+    ds = oracle.Dataset(2, rows)
+    q = np.array([3, 11, 4000], np.int32)
+    r = float(np.float32(oracle.dist(ds, 7, 3, False) * (1 + 1e-6)))
+    with gts.Index(rows, 2, max_h=4) as idx:
+        got = idx.range(q, r, form=gts.FORM_FAST)
+    np.testing.assert_array_equal(got, oracle.range_brute(ds, q, r))
+    assert got[0] >= 1501
