@@ -131,7 +131,7 @@ int main(int argc, char **argv)
         std::vector<int> counts(qnum);
         printf("Searching...\n");
         s = std::chrono::high_resolution_clock::now();
-        if (gts_range(idx, qids, qnum, r, counts.data()) != GTS_OK) die("searchIndexRnnV2");
+        if (gts_range_form(idx, qids, qnum, r, form, counts.data()) != GTS_OK) die("searchIndexRnnV2");
         e = std::chrono::high_resolution_clock::now();
         float time_search = std::chrono::duration<float>(e - s).count();
         for (int i = 0; i < qnum; i++) fprintf(fcost, "%d ", counts[i]);
