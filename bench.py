@@ -15,6 +15,8 @@ One step = one batch of 10,000 queries through the search.  The data set
 
 --k-mix runs the same data with each query's k drawn uniformly from
 {1, 8, 32, 64}: one batch per k per step (the reference takes one k per run).
+--op range times range counts instead, at the --range-quantile (0.001)
+distance quantile of seeded random pairs.
 
 --impl reference times the reference's own CUDA build (oracle/_ref, built
 from the reference sources) through its entry points on the same workload
@@ -125,6 +127,9 @@ def workload(args, rank=0):
     rows = G.gmm_rows(args.n, args.dim, 256, 0.2, seed=args.seed)
     from gts_b200 import replicas as R
     qids = G.query_ids(args.n, args.queries, seed=R.rank_query_seed(args.seed, rank))
+    if args.op == "range":
+        # the radius at the given quantile of seeded random pair distances
+        args.radius = float(np.float32(G.quantile_radius(2, args.range_quantile, 20000, args.seed + 5, rows=rows)))
     return rows, qids
 
 
@@ -142,6 +147,14 @@ def k_groups(args, n_queries):
 
 
 def config_dict(args, world):
+    if args.op == "range":
+        return {"workload": f"gmm{args.n // 1000}k_d{args.dim}_l2_range",
+                "n": args.n, "dim": args.dim, "metric": "L2", "queries_per_gpu": args.queries,
+                "range_quantile": args.range_quantile, "radius": getattr(args, "radius", None),
+                "tree_order": 10, "max_size": 20, "max_h": args.max_h,
+                "form": args.form + (" (bf16 filter, bound fixed at r^2)" if args.form == "fast" else ""),
+                "parallelism": f"query-sharded replicas x{world}",
+                "l2_flush": "no (512 MB data set > 126 MB L2)"}
     return {"workload": f"gmm{args.n // 1000}k_d{args.dim}_l2_knn" + ("_kmix" if args.k_mix else ""),
             "n": args.n, "dim": args.dim, "metric": "L2", "queries_per_gpu": args.queries,
             "k": ("uniform over {1, 8, 32, 64}, one batch per k" if args.k_mix else args.k),
@@ -164,25 +177,28 @@ def run_reference(args):
     if rank != 0:
         return 0
     drv = os.path.join(ROOT, "oracle", "_ref", "gts_ref_driver")
-    base = {"impl": "reference", "metric": "exact kNN queries/s", "unit": "queries/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+    from gts_b200 import datagen as G
+    rows, qids = workload(args)
+    rng = args.op == "range"
+    base = {"impl": "reference", "metric": "exact range queries/s" if rng else "exact kNN queries/s",
+            "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "config": config_dict(args, 1)}
     if not os.path.exists(drv):
         print(json.dumps({**base, "unavailable": "reference CUDA build oracle/_ref/gts_ref_driver is not built"}))
         return 0
-    from gts_b200 import datagen as G
-    rows, qids = workload(args)
-    ref_kth = np.zeros(len(qids), np.float32)
+    ref_kth = np.zeros(len(qids), np.int32 if rng else np.float32)
     t, wall, build_s = 0.0, 0.0, 0.0
     with tempfile.TemporaryDirectory() as tmp:
         dpath = os.path.join(tmp, "data.bin")
         G.write_data_bin(dpath, 2, rows)
         # one reference run per k (it takes one k per run); a step is all of them
-        for k, sel in k_groups(args, len(qids)):
+        groups = [(0, np.arange(len(qids)))] if rng else k_groups(args, len(qids))
+        for k, sel in groups:
             qpath = os.path.join(tmp, f"q{k}.txt")
             G.write_queries(qpath, qids[sel])
             out = os.path.join(tmp, f"res{k}.txt")
-            cmd = [drv, dpath, qpath, "0", str(k), out, "--order", "10", "--max-size", "20",
+            op, param = ("1", repr(args.radius)) if rng else ("0", str(k))
+            cmd = [drv, dpath, qpath, op, param, out, "--order", "10", "--max-size", "20",
                    "--max-h", str(args.max_h), "--budget-gb", "6",
                    "--repeat", str(args.warmup + args.steps)]
             t0 = time.time()
@@ -196,13 +212,15 @@ def run_reference(args):
             info = json.loads(lines[-1])
             t += statistics.mean(info["search_runs"][args.warmup:])
             build_s += info["build_s"]
-            ref_kth[sel] = np.array([float(v) for v in open(out).read().split("\n")[2].split()], np.float32)
+            vals = open(out).read().split("\n")[2].split()
+            ref_kth[sel] = (np.array([int(v) for v in vals], np.int32) if rng
+                            else np.array([float(v) for v in vals], np.float32))
         value = args.queries / t
     line = {**base, "value": value, "ms_per_step": t * 1e3, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian mixture)",
             "build_s": build_s, "wall_s": wall,
             "cpu_baseline": {"value": value, "unit": "queries/s", "cores": 1, "kind": "reference",
-                             "sample": f"reference CUDA build (searchIndexKnnV2) on the B200, "
+                             "sample": f"reference CUDA build ({'searchIndexRnnV2' if rng else 'searchIndexKnnV2'}) on the B200, "
                                        f"{args.queries} queries per step, 6 GB list-table budget; "
                                        f"one host thread drives it"},
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
@@ -214,7 +232,7 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ our arm
 
-def cpu_baseline(rows, qids, groups, sample, kth_gpu):
+def cpu_baseline(rows, qids, groups, sample, kth_gpu, radius=None):
     """Exact multi-threaded brute force (reference leaf arithmetic) on the host,
     on the leading queries of each k batch (sample split evenly)."""
     from oracle import oracle as O
@@ -225,13 +243,17 @@ def cpu_baseline(rows, qids, groups, sample, kth_gpu):
     for g in groups:
         sel = g["sel"][:per]
         t0 = time.perf_counter()
-        kth, _, _ = O.knn_brute(ds, qids[sel], g["k"], nthreads=cores)
+        if radius is not None:
+            kth = O.range_brute(ds, qids[sel], radius, nthreads=cores)
+        else:
+            kth, _, _ = O.knn_brute(ds, qids[sel], g["k"], nthreads=cores)
         dt += time.perf_counter() - t0
         agree += int((kth == kth_gpu[sel]).sum())
         n += len(sel)
     return {"value": n / dt, "unit": "queries/s", "cores": cores, "kind": "port",
             "sample": f"{n} of the {len(qids)} queries, exact brute force over all "
-                      f"{len(rows)} rows in the reference's F64 leaf arithmetic, {cores} threads",
+                      f"{len(rows)} rows in the reference's {'F32 range' if radius is not None else 'F64 kNN'} "
+                      f"leaf arithmetic, {cores} threads",
             "agrees_with_gpu": f"{agree}/{n}"}
 
 
@@ -262,7 +284,10 @@ def run_gts(args):
     del d_rows
     form = {"fast": gts.FORM_FAST, "plain": gts.FORM_PLAIN, "plain-learned": gts.FORM_PLAIN_LEARNED}[args.form]
     learn = None
-    if args.form in ("fast", "plain-learned") and not args.no_learn:
+    rng = args.op == "range"
+    if rng and args.form == "plain-learned":
+        raise SystemExit("--op range takes --form fast or plain")
+    if args.form in ("fast", "plain-learned") and not args.no_learn and not rng:
         # learned radius: 200,000 exact radii from the index itself, trained on
         # the device before the timed region
         torch.cuda.synchronize()
@@ -276,12 +301,16 @@ def run_gts(args):
     groups = []
     for k, sel in k_groups(args, Q):
         groups.append({"k": k, "sel": sel, "q": torch.from_numpy(np.ascontiguousarray(qids[sel])).to(dev),
-                       "kth": torch.empty(len(sel), dtype=torch.float32, device=dev)})
+                       "kth": torch.empty(len(sel), dtype=torch.int32 if rng else torch.float32, device=dev)})
     k = groups[0]["k"] if len(groups) == 1 else None
 
     def run_group(g):
-        idx.knn_device(g["q"].data_ptr(), len(g["sel"]), g["k"], g["kth"].data_ptr(), form=form,
-                       stream=stream.cuda_stream)
+        if rng:
+            idx.range_device(g["q"].data_ptr(), len(g["sel"]), args.radius, g["kth"].data_ptr(),
+                             stream=stream.cuda_stream, form=form)
+        else:
+            idx.knn_device(g["q"].data_ptr(), len(g["sel"]), g["k"], g["kth"].data_ptr(), form=form,
+                           stream=stream.cuda_stream)
 
     def step():
         for g in groups:
@@ -349,7 +378,7 @@ def run_gts(args):
         dist.barrier()
     ms_per_step = total_ms / args.steps
     value = world * Q * args.steps / (total_ms / 1e3)
-    kth_gpu = np.zeros(Q, np.float32)
+    kth_gpu = np.zeros(Q, np.int32 if rng else np.float32)
     for g in groups:
         kth_gpu[g["sel"]] = g["kth"].cpu().numpy()
 
@@ -359,13 +388,14 @@ def run_gts(args):
         g["h_q"] = torch.from_numpy(np.ascontiguousarray(qids[g["sel"]])).pin_memory().numpy()
     for _ in range(max(1, args.warmup)):
         for g in groups:
-            idx.knn(g["h_q"], g["k"], form=form)
+            idx.range(g["h_q"], args.radius, form=form) if rng else idx.knn(g["h_q"], g["k"], form=form)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        kth_e2e = [idx.knn(g["h_q"], g["k"], form=form) for g in groups]
+        kth_e2e = [idx.range(g["h_q"], args.radius, form=form) if rng else idx.knn(g["h_q"], g["k"], form=form)
+                   for g in groups]
     e2e_s = time.perf_counter() - t0
     if world > 1:
         e2e_s = R.max_over_ranks(e2e_s, dist, dev)
@@ -388,8 +418,8 @@ def run_gts(args):
             per_unit = json.load(f)
     if args.form != "fast":
         # every leaf row and pivot row a query reads, plus its own row and result
-        alg_bytes = 4 * d * (stats["objects"] + stats["pivots"]) + sum(len(g["sel"]) * (4 * d + 8 * g["k"])
-                                                                       for g in groups)
+        alg_bytes = 4 * d * (stats["objects"] + stats["pivots"]) + sum(
+            len(g["sel"]) * (4 * d + (4 if rng else 8 * g["k"])) for g in groups)
         achieved = alg_bytes / (launch_ms / 1e3) / 1e9
         traffic = None
         if "k_search" in per_unit:
@@ -428,19 +458,22 @@ def run_gts(args):
                                   "exact_rechecks": stats["exact"] / Q,
                                   "fallback_queries": stats["fallback"], "passes": stats["passes"]},
                     "block_pairs_kept": (stats["blocks"] / stats["tested"]) if stats["tested"] else None}
-    line = {"metric": "exact kNN queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
+    line = {"metric": "exact range queries/s" if rng else "exact kNN queries/s", "value": value,
+            "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32/f64" if args.form != "fast" else "bf16/f32/f64",
             "data": "synthetic (seeded Gaussian mixture; the paper's data sets are absent)",
             "config": config_dict(args, world), "build_s": build_s, "learned_radius": learn,
-            "autotune": ((idx.fast_config(k) if k is not None else {str(g["k"]): idx.fast_config(g["k"])
-                                                                     for g in groups})
-                         if args.form == "fast" else {"threads_per_query_cta": idx.plain_threads(0)}),
+            "autotune": (({"col_groups": 4, "item_blocks": 16, "tuned": False} if rng
+                          else idx.fast_config(k) if k is not None
+                          else {str(g["k"]): idx.fast_config(g["k"]) for g in groups})
+                         if args.form == "fast" else {"threads_per_query_cta": idx.plain_threads(1 if rng else 0)}),
             "roofline": roofline,
             "e2e": e2e, "gpu_launches": launches, "clocks": clock_summary}
     if rank == 0 and world == 1 and args.cpu_sample > 0:
-        line["cpu_baseline"] = cpu_baseline(rows, qids, groups, args.cpu_sample, kth_gpu)
+        line["cpu_baseline"] = cpu_baseline(rows, qids, groups, args.cpu_sample, kth_gpu,
+                                            args.radius if rng else None)
     if rank == 0:
         print(json.dumps(line))
     idx.close()
@@ -462,6 +495,9 @@ def main():
     ap.add_argument("--dim", type=int, default=128)
     ap.add_argument("--queries", type=int, default=10_000)
     ap.add_argument("--k", type=int, default=8)
+    ap.add_argument("--op", choices=["knn", "range"], default="knn",
+                    help="range: range counts at the --range-quantile distance quantile")
+    ap.add_argument("--range-quantile", type=float, default=0.001)
     ap.add_argument("--k-mix", action="store_true",
                     help="k uniform over {1, 8, 32, 64} per query (one batch per k per step)")
     ap.add_argument("--max-h", type=int, default=6)

@@ -2060,10 +2060,14 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
         a.stats = idx->d_stats;
         a.r2lo = r2lo;
         a.rcnt = rcnt;
+        const bool timed = idx->time_filter && idx->fev[0];
+        if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[0], st));
         if ((rc = launch_fast_tile_cg<4, 8, true>(a, nsm, st))) return rc;
+        if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[1], st));
+        k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 1ull);
         k_fast_range_final<<<n, 128, 0, st>>>(idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, dq, r,
                                               rb.cpos, rb.ccnt, rcnt, d_counts + q0, fail, rb.ctr, idx->d_stats);
-        idx->kernel_launches += 10;
+        idx->kernel_launches += 9;   // keys, init, arec, need_sb, need_blk, items, tile, stat, final
         GTS_CUDA_TRY(cudaGetLastError());
         int status = 0, n_fail = 0;
         GTS_CUDA_TRY(cudaMemcpyAsync(&status, idx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -2072,6 +2076,12 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
         if (status != 0) {
             gts_set_error("tensor-core filter kernel reported status %d (barrier wait gave up)", status);
             return GTS_ERR_KERNEL;
+        }
+        if (timed) {
+            float ms = 0.f;
+            GTS_CUDA_TRY(cudaEventElapsedTime(&ms, idx->fev[0], idx->fev[1]));
+            idx->filter_ms += ms;
+            idx->filter_launches++;
         }
         if (n_fail > 0) {
             // overflowed lists: the plain traversal counts those queries

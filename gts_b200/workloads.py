@@ -6,7 +6,8 @@ shapes and distributions), for profiling and smoke runs:
 
 * L2 (Gaussian mixture, 128-d): tree build, filter block order and records,
   learned-radius training and inference, fast kNN, plain kNN (unseeded and
-  seeded by the learned radius), range counts, range ids;
+  seeded by the learned radius), range counts (plain and tensor-core), range
+  ids;
 * edit distance (Zipf words): build, kNN and range;
 * L1 (2-D hotspots): build and range;
 * streaming updates (L2): inserts, deletes and range queries through the
@@ -53,6 +54,8 @@ def run(scale: float = 0.1, seed: int = 11) -> None:
             _t(f"fast kNN k={k}", idx.knn, qids, k, form=gts.FORM_FAST)
         r = float(np.float32(G.quantile_radius(2, 0.001, 20000, seed + 2, rows=rows)))
         counts = _t("range counts", idx.range, qids[: len(plain)], r)
+        fast_counts = _t("range counts, tensor-core filter", idx.range, qids, r, form=gts.FORM_FAST)
+        assert np.array_equal(fast_counts[: len(plain)], counts), "fast and plain range counts differ"
         ids = _t("range ids", idx.range_ids, qids[: len(plain) // 4], r)
         assert np.array_equal(ids[0], counts[: len(plain) // 4]), "range ids and counts differ"
     ne = max(4000, int(1_000_000 * scale))
