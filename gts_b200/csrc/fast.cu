@@ -1942,6 +1942,13 @@ __global__ void k_fast_range_init(int qnum, int *cand_cnt, int *r2_bits, int *rc
 // pow(., 0.5); the query itself at 0) and count when it is within r; the
 // count adds to the objects the filter found certainly inside.  A query
 // whose list overflowed goes to the overflow list.
+//
+// One thread per listed object.  The accumulation uses exact squares (a
+// float difference squared is exact in FP64) in place of pow(e, 2), which
+// is within 2 ulp of it: each step's double sum then differs from the
+// reference's by at most 4.4e-16 (term + sum), so both round to the same
+// float unless the sum lies within that of a float rounding midpoint.  A
+// step that comes that close sends the object through the pow terms.
 __global__ void __launch_bounds__(128) k_fast_range_final(const float *__restrict__ rows, int dim, int num,
                                                           const float *__restrict__ prow, int kp,
                                                           const int *__restrict__ ids_of_slot, int nslots,
@@ -1952,22 +1959,45 @@ __global__ void __launch_bounds__(128) k_fast_range_final(const float *__restric
                                                           int *n_overflow, unsigned long long *stats)
 {
     __shared__ int c;
+    __shared__ float qs[kFMaxKp];
     const int q = blockIdx.x, t = threadIdx.x;
     const int cnt = cand_cnt[q];
     if (cnt > kFCand) {
         if (t == 0) overflow[atomicAdd(n_overflow, 1)] = q;
         return;
     }
-    if (t == 0) c = 0;
-    __syncthreads();
     const int qid = qids[q];
-    const float *qrow = rows + (size_t)qid * dim;
+    if (t == 0) c = 0;
+    for (int j = t; j < dim; j += 128) qs[j] = rows[(size_t)qid * dim + j];
+    __syncthreads();
     for (int i = t; i < cnt; i += 128) {
         const int slot = cand_pos[(size_t)q * kFCand + i];
         if (slot < 0 || slot >= nslots) continue;
         const int id = ids_of_slot[slot];
         if (id < 0 || id >= num) continue;
-        const float d = id == qid ? 0.f : dist_row_f32(prow + (size_t)slot * kp, qrow, dim, kL2);
+        float d = 0.f;
+        if (id != qid) {
+            const float *orow = prow + (size_t)slot * kp;
+            float res = 0.f;
+            bool risky = false;
+#pragma unroll 8
+            for (int j = 0; j < dim; j++) {
+                const double e = (double)(orow[j] - qs[j]);
+                const double tt = e * e;
+                const double s2 = (double)res + tt;
+                const float f = __double2float_rn(s2);
+                const double fd = f;
+                const double nb = (double)__int_as_float(__float_as_int(f) + (s2 > fd ? 1 : -1));
+                const double mid = 0.5 * (fd + nb);
+                if (s2 != fd && fabs(s2 - mid) <= tt * 8.9e-16 + s2 * 4.5e-16) risky = true;
+                res = f;
+            }
+            if (risky) {
+                res = 0.f;
+                for (int j = 0; j < dim; j++) res += pow(orow[j] - qs[j], 2);
+            }
+            d = pow(res, 0.5);
+        }
         if (d <= r) atomicAdd(&c, 1);
     }
     __syncthreads();
