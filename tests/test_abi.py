@@ -96,3 +96,19 @@ def test_no_device_is_a_clean_error():
     with pytest.raises(gts.GtsError) as e:
         gts.Index(np.zeros((10, 4), np.float32), 2)
     assert e.value.code == -2
+
+
+def test_argument_checks_need_no_device():
+    """Entry points reject bad arguments before touching a device."""
+    lib = gts._load_lib()
+    q = np.zeros(4, np.int32)
+    out = np.zeros(4, np.int32)
+    ip = q.ctypes.data_as(C.c_void_p)
+    op = out.ctypes.data_as(C.c_void_p)
+    # null handle, and a form the range entry point does not take
+    assert lib.gts_range_form(None, ip, 4, C.c_float(1.0), 1, op) == -1
+    assert lib.gts_range_form_device(None, ip, 4, C.c_float(1.0), 0, op, None) == -1
+    assert lib.gts_plain_threads_set(None, 0, 256) == -1
+    assert lib.gts_fast_config_set(None, 8, 0, 4, 16) == -1
+    msg = lib.gts_last_error()
+    assert msg
