@@ -286,8 +286,9 @@ __global__ void __launch_bounds__(128) k_fast_arec(const float *__restrict__ row
 // query's own block (the query is one of its objects), widened past every
 // rounding difference to the reference's value, lowers the query's bound.
 // The block's rows are read from the slot-ordered copy (one contiguous
-// 128 x kp range): one warp per row, lane l holding dimensions 4l..4l+3,
-// eight rows in flight per warp.
+// 128 x kp range): one warp per 32 rows, lane l holding dimensions
+// 4l..4l+3, sixteen rows in flight per warp; warp 0 then takes out the
+// smallest value k - 1 times (four values per lane).
 __global__ void __launch_bounds__(128) k_fast_seed(const float *__restrict__ rows, const int *__restrict__ qids,
                                                    FastSummary bs, int dim, int kp, int k, int *__restrict__ r2_bits)
 {
@@ -295,47 +296,56 @@ __global__ void __launch_bounds__(128) k_fast_seed(const float *__restrict__ row
     const int q = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int qid = qids[q];
     const int base = bs.pos[qid] / kFB * kFB;
-    const int cnt = __syncthreads_count(bs.ids[base + t] >= 0);   // valid slots come first
+    const bool valid = bs.ids[base + t] >= 0;   // valid slots come first
+    const int cnt = __syncthreads_count(valid);
     if (cnt < k) return;
+    const unsigned vm = __ballot_sync(0xffffffffu, valid);   // this warp's 32 rows
     const float *qr = rows + (size_t)qid * dim;
     const bool act = 4 * lane < kp;   // kp <= 128
     float qv[4];
 #pragma unroll
     for (int e = 0; e < 4; e++) qv[e] = (act && 4 * lane + e < dim) ? qr[4 * lane + e] : 0.f;
-    const float *pb = bs.prow + (size_t)base * kp + 4 * lane;
-    for (int i0 = 0; i0 < 32; i0 += 8) {
-        float acc[8];
+    const float *pb = bs.prow + (size_t)(base + warp * 32) * kp + 4 * lane;
 #pragma unroll
-        for (int r = 0; r < 8; r++) {
-            const int row = warp * 32 + i0 + r;
+    for (int i0 = 0; i0 < 32; i0 += 16) {
+        float acc[16];
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
             float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (act && row < cnt) o = *reinterpret_cast<const float4 *>(pb + (size_t)row * kp);
+            if (act && ((vm >> (i0 + r)) & 1u)) o = *reinterpret_cast<const float4 *>(pb + (size_t)(i0 + r) * kp);
             const float e0 = o.x - qv[0], e1 = o.y - qv[1], e2 = o.z - qv[2], e3 = o.w - qv[3];
             acc[r] = fmaf(e3, e3, fmaf(e2, e2, fmaf(e1, e1, e0 * e0)));
         }
 #pragma unroll
-        for (int r = 0; r < 8; r++) {
+        for (int r = 0; r < 16; r++) {
             const float s = warp_sum(acc[r]);
-            const int row = warp * 32 + i0 + r;
-            if (lane == 0) v[row] = row < cnt ? s : FLT_MAX;
+            if (lane == 0) v[warp * 32 + i0 + r] = ((vm >> (i0 + r)) & 1u) ? s : FLT_MAX;
         }
     }
     __syncthreads();
-    for (int size = 2; size <= kFB; size <<= 1) {
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            if (t < kFB / 2) {
-                int lo = 2 * t - (t & (stride - 1)), hi = lo + stride;
-                bool up = (lo & size) == 0;
-                float x = v[lo], y = v[hi];
-                if ((x > y) == up) { v[lo] = y; v[hi] = x; }
-            }
-            __syncthreads();
+    if (warp != 0) return;
+    float x[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) x[m] = v[lane + 32 * m];
+    float mn = FLT_MAX;
+    for (int it = 0; it < k; it++) {
+        const float lm = fminf(fminf(x[0], x[1]), fminf(x[2], x[3]));
+        mn = lm;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        if (it == k - 1) break;
+        const unsigned own = __ballot_sync(0xffffffffu, lm == mn);
+        if (lane == __ffs(own) - 1) {
+            if (x[0] == mn) x[0] = FLT_MAX;
+            else if (x[1] == mn) x[1] = FLT_MAX;
+            else if (x[2] == mn) x[2] = FLT_MAX;
+            else x[3] = FLT_MAX;
         }
     }
     // FP32 sum of at most 128 non-negative terms (4 per lane, then a 32-lane
     // tree): relative error < 2^-19 against the reference's FP64 sum of the
     // same FP32 differences
-    if (t == 0) atomicMin(&r2_bits[q], __float_as_int(v[k - 1] * (1.f + 3e-5f)));
+    if (lane == 0) atomicMin(&r2_bits[q], __float_as_int(mn * (1.f + 3e-5f)));
 }
 
 // ---------------------------------------------------------------- pruning
