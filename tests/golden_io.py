@@ -28,8 +28,8 @@ def sample_dir():
     """Directory holding the reference's sample data set, if present here:
     the checkout, or the copy the oracle's reference build stages beside it
     (oracle/_ref/sample, made by `make -C oracle ref`)."""
-    for d in (os.environ.get("GTS_SAMPLE_DIR", ""), "/root/reference/Datasets Sample",
-              os.path.join(GOLDEN, "..", "..", "oracle", "_ref", "sample")):
+    for d in (os.environ.get("GTS_SAMPLE_DIR", ""), os.path.join(GOLDEN, "..", "..", "oracle", "_ref", "sample"),
+              "/root/reference/Datasets Sample"):
         if d and os.path.exists(os.path.join(d, "sbw_example.txt")):
             return d
     return None
