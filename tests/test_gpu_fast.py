@@ -158,3 +158,25 @@ def test_fast_range_overflow_goes_to_the_plain_traversal(oracle):
         got = idx.range(q, r, form=gts.FORM_FAST)
     np.testing.assert_array_equal(got, oracle.range_brute(ds, q, r))
     assert got[0] >= 1501
+
+
+def test_fast_range_extremes_and_device_entry(oracle):
+    """A radius beyond every distance counts every object (all of them
+    certainly inside), a tiny one only the query itself; the device-buffer
+    entry point gives the host one's counts."""
+    import torch
+    rows = G.gmm_rows(6000, 32, 6, 0.5, seed=81)
+    ds = oracle.Dataset(2, rows)
+    q = G.query_ids(6000, 200, seed=82)
+    with gts.Index(rows, 2, max_h=4) as idx:
+        np.testing.assert_array_equal(idx.range(q, 1e6, form=gts.FORM_FAST), np.full(len(q), 6000, np.int32))
+        tiny = idx.range(q, 1e-6, form=gts.FORM_FAST)
+        np.testing.assert_array_equal(tiny, oracle.range_brute(ds, q, 1e-6))
+        r = float(np.float32(G.quantile_radius(2, 0.02, 20000, 83, rows=rows)))
+        host = idx.range(q, r, form=gts.FORM_FAST)
+        d_q = torch.from_numpy(q).cuda()
+        d_c = torch.empty(len(q), dtype=torch.int32, device="cuda")
+        idx.range_device(d_q.data_ptr(), len(q), r, d_c.data_ptr(), form=gts.FORM_FAST)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(d_c.cpu().numpy(), host)
+        np.testing.assert_array_equal(host, oracle.range_brute(ds, q, r))
