@@ -248,6 +248,13 @@ class Index:
         out["tree_h"] = inf["tree_h"]
         return out
 
+    def prepare(self, form: int = FORM_FAST, stream: int = 0) -> bool:
+        """Build the structures `form` needs beyond the tree now (the fast
+        form's filter records); True when the index holds them afterwards."""
+        done = C.c_int()
+        _check(self._lib.gts_index_prepare(self._h, int(form), C.c_void_p(stream), C.byref(done)))
+        return bool(done.value)
+
     def set_stream(self, stream: int):
         _check(self._lib.gts_index_set_stream(self._h, C.c_void_p(stream)))
 
@@ -385,6 +392,29 @@ class Index:
         _check(self._lib.gts_update_run(self._h, _ip(f), _ip(i), len(f), C.c_float(r), _ip(out),
                                         C.byref(nq), C.byref(ts), C.byref(tu)))
         return out[:nq.value], ts.value, tu.value
+
+
+def update_plan(num: int, flags, ids, max_in_size: int = 10) -> dict:
+    """The host pass of the stream update (updateIndexRnn's id bookkeeping,
+    update.cuh:473-623) with no device work: per query op its data row, its
+    operation index and whether the cache list held entries; per entry (the
+    num data rows, then one copy per insert) the row it copies and its
+    (tree_from, tree_to, cache_from, cache_to) operation intervals; the data
+    rows after the last compaction."""
+    f = np.ascontiguousarray(flags, dtype=np.int32)
+    i = np.ascontiguousarray(ids, dtype=np.int32)
+    nq_cap = max(1, int((f == 2).sum()))
+    ne_cap = num + int((f == 0).sum())
+    q_obj, q_time, q_cache = (np.empty(nq_cap, np.int32) for _ in range(3))
+    src = np.empty(ne_cap, np.int32)
+    life = np.empty((ne_cap, 4), np.int32)
+    final = np.empty(max(1, ne_cap), np.int32)
+    nq, ne, nf = C.c_int(), C.c_int(), C.c_int()
+    _check(_load_lib().gts_update_plan(num, _ip(f), _ip(i), len(f), max_in_size, _ip(q_obj), _ip(q_time),
+                                       _ip(q_cache), C.byref(nq), _ip(src), _ip(life), C.byref(ne),
+                                       _ip(final), C.byref(nf)))
+    return {"q_obj": q_obj[:nq.value], "q_time": q_time[:nq.value], "q_cache": q_cache[:nq.value].astype(bool),
+            "ent_src": src[:ne.value], "ent_life": life[:ne.value], "final_rows": final[:nf.value]}
 
 
 # ------------------------------------------------- reference-named wrappers

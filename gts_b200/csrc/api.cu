@@ -433,6 +433,18 @@ extern "C" int gts_kernel_launches(const gts_index *idx, long long *count)
     return GTS_OK;
 }
 
+extern "C" int gts_index_prepare(gts_index *idx, int form, void *stream, int *prepared)
+{
+    if (!idx || (form != GTS_FORM_PLAIN && form != GTS_FORM_FAST && form != GTS_FORM_PLAIN_LEARNED)) {
+        gts_set_error("gts_index_prepare: invalid argument");
+        return GTS_ERR_INVALID;
+    }
+    int done = 0, rc = GTS_OK;
+    if (form == GTS_FORM_FAST) rc = gts::fast_prepare_now(idx, (cudaStream_t)stream, &done);
+    if (prepared) *prepared = done;
+    return rc;
+}
+
 extern "C" int gts_index_set_stream(gts_index *idx, void *stream)
 {
     if (!idx) {

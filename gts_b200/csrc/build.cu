@@ -48,6 +48,7 @@ template int dev_alloc<double>(double **, size_t, size_t *);
 template int dev_alloc<uint32_t>(uint32_t **, size_t, size_t *);
 template int dev_alloc<unsigned short>(unsigned short **, size_t, size_t *);
 template int dev_alloc<unsigned long long>(unsigned long long **, size_t, size_t *);
+template int dev_alloc<int4>(int4 **, size_t, size_t *);
 
 // Build-time distance between two objects (by id), F64 or F32 site.
 __device__ __forceinline__ double obj_dist(const DevData &d, int a, int b, int acc)

@@ -1858,6 +1858,18 @@ static int fast_autotune(gts_index *idx, FastCall &fc, int qc, const int *d_qids
     return rc;
 }
 
+// Build the tensor-core form's block order and filter records now instead of
+// on the first fast search.  *done = 1 when the index holds them afterwards,
+// 0 when the form does not apply to this index (nothing to build).
+int fast_prepare_now(gts_index *idx, cudaStream_t st, int *done)
+{
+    *done = 0;
+    if (!fast_supported(idx, 1)) return GTS_OK;
+    int rc = fast_prepare(idx, st);
+    if (rc == GTS_OK) *done = 1;
+    return rc;
+}
+
 int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                     float *d_dists, cudaStream_t st)
 {

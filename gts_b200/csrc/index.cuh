@@ -100,6 +100,13 @@ int search_knn(gts_index *idx, const int *d_qids, int qnum, int k, int form,
 int search_range(gts_index *idx, const int *d_qids, int qnum, float r, int *d_counts,
                  const uint32_t *d_deleted, cudaStream_t s);
 int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int *d_counts, cudaStream_t s);
+// Range counts at time stamps (the stream-update path): query q is object
+// d_qids[q] at operation d_qtime[q]; an object within r adds its entries
+// live in the tree (d_tree_counts) and in the cache list (d_cache_counts)
+// at that operation (SearchArgs::ents).
+int search_range_timed(gts_index *idx, const int *d_qids, const int *d_qtime, int qnum, float r,
+                       const int *d_ent_off, const int4 *d_ents, int *d_tree_counts, int *d_cache_counts,
+                       cudaStream_t s);
 int search_range_ids(gts_index *idx, const int *d_qids, int qnum, float r, int *d_counts,
                      int *d_ids, float *d_dists, const int *d_offsets, cudaStream_t s);
 
@@ -118,6 +125,7 @@ int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d
 int search_knn_plain_learned(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                              float *d_dists, cudaStream_t s);
 int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *cg, int *item);
+int fast_prepare_now(gts_index *idx, cudaStream_t st, int *done);
 // Drop the captured filter graph (its device pointers or parameters changed).
 void graph_invalidate(gts_index *idx);
 // Unseeded filter with all scratch inside the caller's fixed buffer.

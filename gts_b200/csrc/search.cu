@@ -25,8 +25,11 @@
 //     with a bitonic sort that keeps the k best and tightens the radius.
 //
 // The query object itself is at distance 0 (search_v2.cuh:338-340,
-// 454-456).  Deleted objects (update path) are skipped
-// (update.cuh:244).  Objects of every childless node are verified, at any
+// 454-456).  Deleted objects (a deletion bitmap) are skipped
+// (update.cuh:244).  The stream-update path counts with time stamps instead
+// (kModeRangeTimed): an object within r adds the number of its entries that
+// are live in the tree, and separately in the cache list, at the query's
+// operation index.  Objects of every childless node are verified, at any
 // depth, so results equal the exact answer for every tree shape.
 #include <algorithm>
 #include <cfloat>
@@ -46,7 +49,7 @@ constexpr int kCandCap = kLeafObjCap + kMaxK;
 constexpr int kSortCap = 2048;        // next power of two >= kCandCap
 constexpr int kMaxDimSmem = 1024;
 
-enum SearchMode { kModeKnn = 0, kModeRangeCount = 1, kModeRangeIds = 2 };
+enum SearchMode { kModeKnn = 0, kModeRangeCount = 1, kModeRangeIds = 2, kModeRangeTimed = 3 };
 
 struct SearchArgs {
     DevTree t;
@@ -71,6 +74,15 @@ struct SearchArgs {
     const int *seed_r2_bits;
     int *fail, *n_fail;
     unsigned long long *stats;   // [objects filtered, pivots evaluated, exact values, queries]
+    // kModeRangeTimed: the query's operation index; per object id its
+    // entries ents[ent_off[id] .. ent_off[id + 1]) as (tree_from, tree_to,
+    // cache_from, cache_to), live in the tree at t when tree_from < t <
+    // tree_to and in the cache list when cache_from < t < cache_to; counts
+    // receives the tree part, counts2 the cache part
+    const int *qtime;
+    const int *ent_off;
+    const int4 *ents;
+    int *counts2;
     float rel_eps;   // relative pruning slack
     float abs_eps;   // absolute pruning slack
 };
@@ -93,7 +105,7 @@ struct __align__(16) SearchSmem {
     int leaf_pre[kBatch + 1];  // prefix of their sizes
     int cpos[kLeafObjCap];     // positions needing an exact value
     int nint, nleaf, ncpos;
-    int top, ncand, q, qid, cnt, overflow;
+    int top, ncand, q, qid, cnt, cnt2, tq, overflow;
     unsigned long long n_obj, n_piv, n_exact;
     double R;
 };
@@ -103,6 +115,21 @@ struct __align__(16) SearchSmem {
 __device__ __forceinline__ bool is_deleted(const uint32_t *bm, int id)
 {
     return bm && ((bm[id >> 5] >> (id & 31)) & 1u);
+}
+
+// kModeRangeTimed: adds object id's entries live in the tree / in the cache
+// list at operation t to the query's two counts.
+__device__ __forceinline__ void add_timed(const SearchArgs &a, SearchSmem &s, int id)
+{
+    const int t = s.tq;
+    int wt = 0, wc = 0;
+    for (int e = a.ent_off[id], e1 = a.ent_off[id + 1]; e < e1; e++) {
+        const int4 v = a.ents[e];
+        wt += (v.x < t && t < v.y) ? 1 : 0;
+        wc += (v.z < t && t < v.w) ? 1 : 0;
+    }
+    if (wt) atomicAdd(&s.cnt, wt);
+    if (wc) atomicAdd(&s.cnt2, wc);
 }
 
 // Exact leaf value, in the reference's arithmetic for the call site.
@@ -315,6 +342,8 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int O = t.order;
     const bool knn = a.mode == kModeKnn;
+    const bool timed = a.mode == kModeRangeTimed;
+    const bool count_only = a.mode == kModeRangeCount || timed;
     const int acc = knn ? kAccF64 : kAccF32;
     const bool warp_filter = (t.metric == kL2 || t.metric == kL1 || t.metric == kLinf);
 
@@ -328,7 +357,8 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
             if (tid == 0) {
                 atomicMax(a.status, (int)kKsBadQuery);
                 if (a.mode == kModeKnn) a.kth[q] = __int_as_float(0x7fc00000);
-                else if (a.mode == kModeRangeCount) a.counts[q] = -1;
+                else if (count_only) a.counts[q] = -1;
+                if (timed) a.counts2[q] = -1;
             }
             __syncthreads();
             continue;
@@ -342,6 +372,8 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
             s.stack_lb[0] = 0.f;
             s.ncand = 0;
             s.cnt = 0;
+            s.cnt2 = 0;
+            s.tq = timed ? a.qtime[q] : 0;
             s.overflow = 0;
             s.n_obj = s.n_piv = s.n_exact = 0;
             s.R = !knn ? (double)a.r
@@ -470,8 +502,9 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
                             if (my_id == qid) lo = hi = 0.f;
                             if (knn) {
                                 if ((double)lo <= s.R) s.cpos[atomicAdd(&s.ncpos, 1)] = my_pos;
-                            } else if (a.mode == kModeRangeCount && (double)hi < (double)a.r * (1.0 - 2.4e-7)) {
-                                atomicAdd(&s.cnt, 1);
+                            } else if (count_only && (double)hi < (double)a.r * (1.0 - 2.4e-7)) {
+                                if (timed) add_timed(a, s, my_id);
+                                else atomicAdd(&s.cnt, 1);
                             } else if ((double)lo <= (double)a.r * (1.0 + 2.4e-7)) {
                                 s.cpos[atomicAdd(&s.ncpos, 1)] = my_pos;
                             }
@@ -501,6 +534,8 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
                             s.cd[slot] = d;
                             s.cid[slot] = id;
                         }
+                    } else if ((float)d <= a.r && timed) {
+                        add_timed(a, s, id);
                     } else if ((float)d <= a.r) {
                         int slot = atomicAdd(&s.cnt, 1);
                         if (a.mode == kModeRangeIds) {
@@ -580,7 +615,8 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
             }
             if (tid == 0 && k > 0) a.kth[q] = s.ncand >= k ? (float)s.cd[k - 1] : (float)t.infi_dis;
         } else if (tid == 0) {
-            if (a.mode == kModeRangeCount) a.counts[q] = s.cnt;
+            if (count_only) a.counts[q] = s.cnt;
+            if (timed) a.counts2[q] = s.cnt2;
         }
         if (tid == 0) {
             if (s.overflow) atomicMax(a.status, (int)kKsStackOverflow);
@@ -730,11 +766,12 @@ static int run_search(gts_index *idx, SearchArgs &a, cudaStream_t st)
     if (!idx->keep_stats) GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, kStatsN * sizeof(unsigned long long), st));
     // threads per query CTA: tuned per search mode on the first batch large
     // enough for plain_autotune's sample, else the tuned or default value
-    int nt = idx->plain_nt[a.mode];
+    const int slot = a.mode == kModeRangeTimed ? kModeRangeCount : a.mode;
+    int nt = idx->plain_nt[slot];
     if (!nt && !idx->keep_stats) {
         int rc = plain_autotune(idx, a, st, &nt);
         if (rc) return rc;
-        if (a.mode != kModeRangeIds) idx->plain_nt[a.mode] = nt;
+        if (a.mode != kModeRangeIds) idx->plain_nt[slot] = nt;
     }
     if (!nt) nt = kPlainDefaultThreads;
     int rc = launch_search(idx, a, nt, st);
@@ -859,6 +896,23 @@ int search_range(gts_index *idx, const int *d_qids, int qnum, float r, int *d_co
     a.r = r;
     a.counts = d_counts;
     a.deleted = d_deleted;
+    return run_search(idx, a, st);
+}
+
+int search_range_timed(gts_index *idx, const int *d_qids, const int *d_qtime, int qnum, float r,
+                       const int *d_ent_off, const int4 *d_ents, int *d_tree_counts, int *d_cache_counts,
+                       cudaStream_t st)
+{
+    SearchArgs a{};
+    a.qids = d_qids;
+    a.qnum = qnum;
+    a.mode = kModeRangeTimed;
+    a.r = r;
+    a.counts = d_tree_counts;
+    a.counts2 = d_cache_counts;
+    a.qtime = d_qtime;
+    a.ent_off = d_ent_off;
+    a.ents = d_ents;
     return run_search(idx, a, st);
 }
 

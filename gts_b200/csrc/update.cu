@@ -16,12 +16,27 @@
 //     cache entries within r (search_naive.cuh:208-251).  When the cache is
 //     empty the cache count of the previous query is reused, as the
 //     reference's rnum is (update.cuh:592-597).
-// What is different: the logical->physical map is a Fenwick tree on the
-// host (O(log N) per delete instead of a device scan), deletions reach the
-// device as a bitmap that the search kernel skips, and each run of
-// consecutive queries is one batched launch.
+//
+// How it runs here.  An insert copies an existing row, so every object that
+// ever exists in the stream is a copy of a row of the data the index was
+// built on.  One host pass over the operations (O(log N) each, two Fenwick
+// trees) keeps the reference's id bookkeeping and gives every entry -- the
+// original rows and every inserted copy -- the operation intervals during
+// which it is live in the tree and in the cache list; it gives every query
+// its object and operation index.  All queries of the stream then run as ONE
+// batched launch of the range traversal over the unchanged tree
+// (kModeRangeTimed, search.cu): an object within r adds its entries live at
+// the query's operation.  The per-query cache counts, with the reference's
+// stale count for an empty cache, are combined on the host.  Physical ids
+// follow from store order: the data array after a compaction is exactly the
+// entries live at that compaction, in store order (original rows first, then
+// the copies in insertion order).  The compactions themselves therefore cost
+// no rebuild; one rebuild at the end leaves the handle holding the data of
+// the last compaction, as the reference's does.  Results are identical to
+// running the rebuilds, since every count is exact.
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <vector>
 #include "index.cuh"
 
@@ -47,36 +62,18 @@ __global__ void k_gather_strs(int n_new, const int *map, const char *src, const 
     }
 }
 
-// Cache-list scan (searchD / searchS, search_naive.cuh:24-127): F32-site
-// distance from every query of the batch to every cached row.
-__global__ void k_cache_scan(DevData d, const int *cache, int in_size, const int *qids, int nq, float r,
-                             int *counts)
-{
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nq * in_size) return;
-    int qi = t / in_size, e = t % in_size;
-    int a = cache[e], b = qids[qi];
-    float res;
-    if (d.metric == kEdit) {
-        res = (float)edit_dp(d.strs + (size_t)a * kStrStride, d.lens[a], d.strs + (size_t)b * kStrStride,
-                             d.lens[b]);
-    } else {
-        res = dist_row_f32(d.rows + (size_t)a * d.dim, d.rows + (size_t)b * d.dim, d.dim, d.metric);
-    }
-    if (res <= r) atomicAdd(&counts[qi], 1);
-}
-
 namespace {
 
-struct Fenwick {   // counts of live tree rows
+// Counts over [0, cap): the first n_live positions start at 1.
+struct Fenwick {
     std::vector<int> t;
     int n = 0, log = 0;
-    void init_all_live(int n_)
+    void init(int cap, int n_live)
     {
-        n = n_;
+        n = cap;
         t.assign((size_t)n + 1, 0);
         for (int i = 1; i <= n; i++) {
-            t[i] += 1;
+            if (i <= n_live) t[i] += 1;
             int j = i + (i & -i);
             if (j <= n) t[j] += t[i];
         }
@@ -87,7 +84,14 @@ struct Fenwick {   // counts of live tree rows
     {
         for (i++; i <= n; i += i & -i) t[i] += v;
     }
-    // physical index of the (u+1)-th live row; caller checks u < live count
+    // sum over [0, i)
+    int prefix(int i) const
+    {
+        int r = 0;
+        for (; i > 0; i -= i & -i) r += t[i];
+        return r;
+    }
+    // position of the (u+1)-th counted position; caller checks u < total
     int select(int u) const
     {
         int pos = 0, rem = u + 1;
@@ -98,7 +102,7 @@ struct Fenwick {   // counts of live tree rows
                 rem -= t[np];
             }
         }
-        return pos;   // 0-based index of the row
+        return pos;
     }
 };
 
@@ -118,22 +122,112 @@ struct DevScratch {
     }
 };
 
+constexpr int kNever = INT_MAX;
+
 }  // namespace
 
-static int rebuild(gts_index *idx, const std::vector<uint8_t> &deleted, const std::vector<int> &cache,
-                   cudaStream_t s)
+// The outcome of the host pass over an update stream.
+struct StreamPlan {
+    std::vector<int> src;      // per entry: the row of the built data it copies
+    std::vector<int4> life;    // per entry: (tree_from, tree_to, cache_from, cache_to)
+    std::vector<int> q_obj, q_time;
+    std::vector<uint8_t> q_cache;   // the cache list was non-empty at the query
+    std::vector<int> final_rows;    // data after the last compaction (empty: none)
+};
+
+// The reference's bookkeeping of update.cuh:473-623 over entries in store
+// order.  fphys counts the entries live at the last compaction (their rank
+// is the physical id); flive the tree entries live now (their rank is the
+// logical id of a delete).
+int plan_stream(int n0, const int *flags, const int *ids, int nops, int max_in, StreamPlan *P)
 {
-    const int tree_size = idx->num;
-    std::vector<int> map;
-    map.reserve((size_t)tree_size + cache.size());
-    for (int j = 0; j < tree_size; j++)
-        if (!deleted[j]) map.push_back(j);
-    for (int c : cache) map.push_back(c);
-    const int n_new = (int)map.size();
-    if (n_new < 1) {
-        gts_set_error("update stream deleted every object");
-        return GTS_ERR_INVALID;
+    int n_ins = 0;
+    for (int i = 0; i < nops; i++) n_ins += flags[i] == 0;
+    const int cap = n0 + n_ins;
+    P->src.resize((size_t)n0);
+    for (int i = 0; i < n0; i++) P->src[i] = i;
+    P->src.reserve((size_t)cap);
+    P->life.assign((size_t)n0, make_int4(-1, kNever, kNever, kNever));
+    P->life.reserve((size_t)cap);
+    Fenwick fphys, flive;
+    fphys.init(cap, n0);
+    flive.init(cap, n0);
+    int tree_size = n0, ndel = 0, delete_id = 0;
+    bool compacted = false;
+    std::vector<int> cache, pending;
+    for (int i = 0; i < nops; i++) {
+        const int f = flags[i];
+        if (f == 0) {   // insert: a copy of physical row ids[i] joins the cache list
+            if (ids[i] >= tree_size) {
+                gts_set_error("op %d inserts row %d, data has %d rows", i, ids[i], tree_size);
+                return GTS_ERR_INVALID;
+            }
+            const int e = (int)P->src.size();
+            P->src.push_back(P->src[fphys.select(ids[i])]);
+            P->life.push_back(make_int4(kNever, kNever, i, kNever));
+            cache.push_back(e);
+            if ((int)cache.size() == max_in) {   // compaction (update.cuh:484-540)
+                for (int p : pending) fphys.add(p, -1);
+                for (int c : cache) {
+                    P->life[c].x = i;   // in the tree from here on
+                    P->life[c].w = i;   // out of the cache list
+                    fphys.add(c, 1);
+                    flive.add(c, 1);
+                }
+                tree_size = tree_size - ndel + (int)cache.size();
+                ndel = 0;
+                cache.clear();
+                pending.clear();
+                compacted = true;
+            }
+        } else if (f == 1) {   // delete (update.cuh:546-582)
+            const int u = ids[i];
+            const int live_tree = tree_size - ndel;
+            if (u >= 0 && u < live_tree) delete_id = fphys.prefix(flive.select(u));
+            else if (u >= live_tree && u < live_tree + (int)cache.size()) delete_id = tree_size + (u - live_tree);
+            if (delete_id < tree_size) {
+                const int e = fphys.select(delete_id);
+                if (P->life[e].y == kNever) {
+                    P->life[e].y = i;
+                    flive.add(e, -1);
+                    pending.push_back(e);
+                    ndel++;
+                }
+            } else if (!cache.empty()) {
+                size_t c = (size_t)(delete_id - tree_size);
+                if (c >= cache.size()) c = cache.size() - 1;
+                P->life[cache[c]].w = i;
+                cache.erase(cache.begin() + (long)c);
+            }
+        } else {   // query: physical row ids[i] (update.cuh:588)
+            const int q = ids[i];
+            if (q < 0 || q >= tree_size) {
+                gts_set_error("update query id %d out of range [0, %d)", q, tree_size);
+                return GTS_ERR_INVALID;
+            }
+            P->q_obj.push_back(P->src[fphys.select(q)]);
+            P->q_time.push_back(i);
+            P->q_cache.push_back(cache.empty() ? 0 : 1);
+        }
     }
+    P->final_rows.clear();
+    if (compacted) {
+        P->final_rows.reserve((size_t)tree_size);
+        for (int e = 0; e < (int)P->src.size(); e++)
+            if (fphys.prefix(e + 1) - fphys.prefix(e)) P->final_rows.push_back(P->src[e]);
+        if (P->final_rows.empty()) {
+            gts_set_error("update stream deleted every object");
+            return GTS_ERR_INVALID;
+        }
+    }
+    return GTS_OK;
+}
+
+// The data after the last compaction (rows `map` of the current data, in
+// order), and the index rebuilt on it.
+static int rebuild_on(gts_index *idx, const std::vector<int> &map, cudaStream_t s)
+{
+    const int n_new = (int)map.size();
     DevScratch sc;
     int *d_map = nullptr;
     int rc;
@@ -170,124 +264,53 @@ int update_run(gts_index *idx, const int *flags, const int *ids, int nops, float
 {
     using clk = std::chrono::high_resolution_clock;
     cudaStream_t s = idx->stream;
-    const int max_in = idx->params.max_in_size;
-    double t_search = 0, t_update = 0;
     auto t0 = clk::now();
-
-    int tree_size = idx->num, ndel = 0, rnum = 0, delete_id = 0, nq = 0;
-    std::vector<int> cache;
-    std::vector<uint8_t> deleted((size_t)tree_size, 0);
-    std::vector<uint32_t> bitmap(((size_t)tree_size + 31) / 32, 0);
-    Fenwick fw;
-    fw.init_all_live(tree_size);
-
-    DevScratch sc;
-    uint32_t *d_bitmap = nullptr;
-    int *d_q = nullptr, *d_cnt = nullptr, *d_ccnt = nullptr, *d_cache = nullptr;
-    int rc;
-    // query batches are bounded by the number of query ops
-    int max_batch = 0;
-    for (int i = 0; i < nops; i++) max_batch += flags[i] == 2;
-    max_batch = std::max(1, std::min(max_batch, 65536));
-    if ((rc = sc.alloc(&d_q, (size_t)max_batch)) || (rc = sc.alloc(&d_cnt, (size_t)max_batch)) ||
-        (rc = sc.alloc(&d_ccnt, (size_t)max_batch)) || (rc = sc.alloc(&d_cache, (size_t)max_in + 1)))
-        return rc;
-    size_t bm_cap = bitmap.size();
-    if ((rc = sc.alloc(&d_bitmap, bm_cap + 1))) return rc;
-    GTS_CUDA_TRY(cudaMemsetAsync(d_bitmap, 0, sizeof(uint32_t) * (bm_cap + 1), s));
-    bool bitmap_dirty = false;
-    std::vector<int> qbuf, cbuf, ccbuf;
-    t_update += std::chrono::duration<double>(clk::now() - t0).count();
-
-    int i = 0;
-    while (i < nops) {
-        int f = flags[i];
-        if (f == 0) {   // insert
-            auto ts = clk::now();
-            if (ids[i] >= tree_size) {
-                gts_set_error("op %d inserts row %d, data has %d rows", i, ids[i], tree_size);
-                return GTS_ERR_INVALID;
-            }
-            cache.push_back(ids[i]);
-            if ((int)cache.size() == max_in) {
-                if ((rc = rebuild(idx, deleted, cache, s))) return rc;
-                tree_size = idx->num;
-                ndel = 0;
-                cache.clear();
-                deleted.assign((size_t)tree_size, 0);
-                bitmap.assign(((size_t)tree_size + 31) / 32, 0);
-                fw.init_all_live(tree_size);
-                if (bitmap.size() > bm_cap) {
-                    cudaFree(d_bitmap);
-                    sc.ps.erase(std::find(sc.ps.begin(), sc.ps.end(), (void *)d_bitmap));
-                    bm_cap = bitmap.size();
-                    if ((rc = sc.alloc(&d_bitmap, bm_cap + 1))) return rc;
-                }
-                GTS_CUDA_TRY(cudaMemsetAsync(d_bitmap, 0, sizeof(uint32_t) * (bm_cap + 1), s));
-                bitmap_dirty = false;
-            }
-            t_update += std::chrono::duration<double>(clk::now() - ts).count();
-            i++;
-        } else if (f == 1) {   // delete
-            auto ts = clk::now();
-            int u = ids[i];
-            int live_tree = tree_size - ndel;
-            if (u >= 0 && u < live_tree) delete_id = fw.select(u);
-            else if (u >= live_tree && u < live_tree + (int)cache.size()) delete_id = tree_size + (u - live_tree);
-            if (delete_id < tree_size) {
-                if (!deleted[delete_id]) {
-                    deleted[delete_id] = 1;
-                    bitmap[delete_id >> 5] |= 1u << (delete_id & 31);
-                    fw.add(delete_id, -1);
-                    ndel++;
-                    bitmap_dirty = true;
-                }
-            } else if (!cache.empty()) {
-                size_t e = (size_t)(delete_id - tree_size);
-                if (e < cache.size()) cache.erase(cache.begin() + (long)e);
-                else cache.pop_back();
-            }
-            t_update += std::chrono::duration<double>(clk::now() - ts).count();
-            i++;
-        } else {   // a run of consecutive queries: one batched launch
-            auto ts = clk::now();
-            qbuf.clear();
-            while (i < nops && flags[i] == 2 && (int)qbuf.size() < max_batch) {
-                int q = ids[i++];
-                if (q < 0 || q >= tree_size) {
-                    gts_set_error("update query id %d out of range [0, %d)", q, tree_size);
-                    return GTS_ERR_INVALID;
-                }
-                qbuf.push_back(q);
-            }
-            const int nb = (int)qbuf.size();
-            if (bitmap_dirty) {
-                GTS_CUDA_TRY(cudaMemcpyAsync(d_bitmap, bitmap.data(), sizeof(uint32_t) * bitmap.size(),
-                                             cudaMemcpyHostToDevice, s));
-                bitmap_dirty = false;
-            }
-            GTS_CUDA_TRY(cudaMemcpyAsync(d_q, qbuf.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
-            if ((rc = search_range(idx, d_q, nb, r, d_cnt, d_bitmap, s))) return rc;
-            cbuf.resize(nb);
-            GTS_CUDA_TRY(cudaMemcpyAsync(cbuf.data(), d_cnt, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
-            const int in_size = (int)cache.size();
-            if (in_size > 0) {
-                GTS_CUDA_TRY(cudaMemcpyAsync(d_cache, cache.data(), sizeof(int) * in_size, cudaMemcpyHostToDevice, s));
-                GTS_CUDA_TRY(cudaMemsetAsync(d_ccnt, 0, sizeof(int) * nb, s));
-                DevData dd{idx->dim, idx->num, idx->metric, idx->rows, idx->strs, idx->lens};
-                int work = nb * in_size;
-                k_cache_scan<<<(work + 127) / 128, 128, 0, s>>>(dd, d_cache, in_size, d_q, nb, r, d_ccnt);
-                GTS_CUDA_TRY(cudaGetLastError());
-                ccbuf.resize(nb);
-                GTS_CUDA_TRY(cudaMemcpyAsync(ccbuf.data(), d_ccnt, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
-            }
-            GTS_CUDA_TRY(cudaStreamSynchronize(s));
-            for (int j = 0; j < nb; j++) {
-                if (in_size > 0) rnum = ccbuf[j];
-                counts_out[nq++] = cbuf[j] + rnum;
-            }
-            t_search += std::chrono::duration<double>(clk::now() - ts).count();
+    StreamPlan P;
+    int rc = plan_stream(idx->num, flags, ids, nops, idx->params.max_in_size, &P);
+    if (rc) return rc;
+    const int nq = (int)P.q_obj.size();
+    double t_update = std::chrono::duration<double>(clk::now() - t0).count();
+    double t_search = 0;
+    if (nq > 0) {
+        auto ts = clk::now();
+        // entries grouped by the row they copy (CSR over the built data)
+        const int n0 = idx->num;
+        const size_t ne = P.src.size();
+        std::vector<int> off((size_t)n0 + 1, 0);
+        for (size_t e = 0; e < ne; e++) off[(size_t)P.src[e] + 1]++;
+        for (int i = 0; i < n0; i++) off[(size_t)i + 1] += off[i];
+        std::vector<int4> ents(ne);
+        {
+            std::vector<int> fill(off.begin(), off.end() - 1);
+            for (size_t e = 0; e < ne; e++) ents[(size_t)fill[P.src[e]]++] = P.life[e];
         }
+        DevScratch sc;
+        int *d_off = nullptr, *d_q = nullptr, *d_t = nullptr, *d_ct = nullptr, *d_cc = nullptr;
+        int4 *d_ents = nullptr;
+        if ((rc = sc.alloc(&d_off, off.size())) || (rc = sc.alloc(&d_ents, ne)) ||
+            (rc = sc.alloc(&d_q, (size_t)nq)) || (rc = sc.alloc(&d_t, (size_t)nq)) ||
+            (rc = sc.alloc(&d_ct, (size_t)nq)) || (rc = sc.alloc(&d_cc, (size_t)nq)))
+            return rc;
+        GTS_CUDA_TRY(cudaMemcpyAsync(d_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, s));
+        GTS_CUDA_TRY(cudaMemcpyAsync(d_ents, ents.data(), sizeof(int4) * ne, cudaMemcpyHostToDevice, s));
+        GTS_CUDA_TRY(cudaMemcpyAsync(d_q, P.q_obj.data(), sizeof(int) * nq, cudaMemcpyHostToDevice, s));
+        GTS_CUDA_TRY(cudaMemcpyAsync(d_t, P.q_time.data(), sizeof(int) * nq, cudaMemcpyHostToDevice, s));
+        if ((rc = search_range_timed(idx, d_q, d_t, nq, r, d_off, d_ents, d_ct, d_cc, s))) return rc;
+        std::vector<int> ct((size_t)nq), cc((size_t)nq);
+        GTS_CUDA_TRY(cudaMemcpyAsync(ct.data(), d_ct, sizeof(int) * nq, cudaMemcpyDeviceToHost, s));
+        GTS_CUDA_TRY(cudaMemcpyAsync(cc.data(), d_cc, sizeof(int) * nq, cudaMemcpyDeviceToHost, s));
+        GTS_CUDA_TRY(cudaStreamSynchronize(s));
+        int rnum = 0;   // the cache count of the last query that had a cache (update.cuh:592-597)
+        for (int j = 0; j < nq; j++) {
+            if (P.q_cache[j]) rnum = cc[j];
+            counts_out[j] = ct[j] + rnum;
+        }
+        t_search = std::chrono::duration<double>(clk::now() - ts).count();
+    }
+    if (!P.final_rows.empty()) {
+        auto tr = clk::now();
+        if ((rc = rebuild_on(idx, P.final_rows, s))) return rc;
+        t_update += std::chrono::duration<double>(clk::now() - tr).count();
     }
     if (nq_out) *nq_out = nq;
     if (search_s) *search_s = t_search;
@@ -296,6 +319,45 @@ int update_run(gts_index *idx, const int *flags, const int *ids, int nops, float
 }
 
 }  // namespace gts
+
+extern "C" int gts_update_plan(int num, const int *flags, const int *ids, int nops, int max_in_size, int *q_obj,
+                               int *q_time, int *q_cache, int *n_q, int *ent_src, int *ent_life, int *n_ent,
+                               int *final_rows, int *n_final)
+{
+    if (num < 1 || nops < 0 || max_in_size < 1 || (nops > 0 && (!flags || !ids)) || !n_q || !n_ent || !n_final) {
+        gts_set_error("gts_update_plan: invalid argument");
+        return GTS_ERR_INVALID;
+    }
+    for (int i = 0; i < nops; i++) {
+        if (flags[i] < 0 || flags[i] > 2 || (flags[i] == 0 && ids[i] < 0)) {
+            gts_set_error("op %d is (%d, %d)", i, flags[i], ids[i]);
+            return GTS_ERR_INVALID;
+        }
+    }
+    gts::StreamPlan P;
+    int rc = gts::plan_stream(num, flags, ids, nops, max_in_size, &P);
+    if (rc) return rc;
+    *n_q = (int)P.q_obj.size();
+    *n_ent = (int)P.src.size();
+    *n_final = (int)P.final_rows.size();
+    for (size_t j = 0; j < P.q_obj.size(); j++) {
+        if (q_obj) q_obj[j] = P.q_obj[j];
+        if (q_time) q_time[j] = P.q_time[j];
+        if (q_cache) q_cache[j] = P.q_cache[j];
+    }
+    for (size_t e = 0; e < P.src.size(); e++) {
+        if (ent_src) ent_src[e] = P.src[e];
+        if (ent_life) {
+            ent_life[4 * e + 0] = P.life[e].x;
+            ent_life[4 * e + 1] = P.life[e].y;
+            ent_life[4 * e + 2] = P.life[e].z;
+            ent_life[4 * e + 3] = P.life[e].w;
+        }
+    }
+    if (final_rows)
+        for (size_t i = 0; i < P.final_rows.size(); i++) final_rows[i] = P.final_rows[i];
+    return GTS_OK;
+}
 
 extern "C" int gts_update_run(gts_index *idx, const int *flags, const int *ids, int nops, float r,
                               int *counts_out, int *nq_out, double *search_s, double *update_s)

@@ -109,6 +109,15 @@ int gts_index_export(const gts_index *idx, int *id_list, int *pid, float *min_di
 
 void gts_index_free(gts_index *idx);
 
+/* No counterpart in the reference (its only index is the tree).  Build
+ * what a search form needs beyond the tree now, on `stream`, instead of in
+ * the first search of that form: for GTS_FORM_FAST on an L2 index with
+ * dim <= 128, the block order, filter records and slot-ordered rows (their
+ * bytes join gts_index_info.device_bytes).  *prepared (nullable) = 1 when
+ * the index holds them afterwards, 0 when the form needs nothing more on
+ * this index.  A rebuild or update drops them again. */
+int gts_index_prepare(gts_index *idx, int form, void *stream, int *prepared);
+
 /* Set the stream used by the host-buffer entry points of this handle. */
 int gts_index_set_stream(gts_index *idx, void *stream);
 
@@ -257,12 +266,33 @@ int gts_radius_model_grad(const float *X, const float *target, int batch, const 
 
 /* updateIndexRnn (update.cuh:449-638): replay a stream of operations
  * (flag 0 insert, 1 delete, 2 range query of radius r) through the lazy
- * cache list of params->max_in_size entries, rebuilding the index when the
- * cache fills.  counts_out receives one entry per query op (*nq_out of
- * them; size it to the number of flag-2 ops).  The index handle is updated
- * in place (it holds the rebuilt tree afterwards). */
+ * cache list of params->max_in_size entries with the reference's id rules
+ * and answers.  counts_out receives one entry per query op (*nq_out of
+ * them; size it to the number of flag-2 ops).  Every query of the stream
+ * runs in one batched launch over the index as it was built (an insert
+ * copies an existing row, so no compaction needs a rebuild); afterwards the
+ * handle holds the data of the last compaction and its rebuilt tree, as the
+ * reference's does.  *search_s: the batched search (copies included);
+ * *update_s: the host pass and the final rebuild. */
 int gts_update_run(gts_index *idx, const int *flags, const int *ids, int nops, float r,
                    int *counts_out, int *nq_out, double *search_s, double *update_s);
+
+/* updateIndexRnn's bookkeeping (update.cuh:473-623) without the device:
+ * the host pass of gts_update_run.  Every object the stream ever holds is
+ * an entry: the num rows of the data (entries 0..num-1) and one copy per
+ * insert, in insertion order.  ent_src[e] is the data row entry e copies;
+ * ent_life[4e..4e+3] = (tree_from, tree_to, cache_from, cache_to): entry e
+ * is in the tree at operation t when tree_from < t < tree_to and in the
+ * cache list when cache_from < t < cache_to (INT_MAX = never).  Query op j
+ * (in stream order) asks about data row q_obj[j] at operation q_time[j];
+ * q_cache[j] = 1 when the cache list was not empty then (otherwise the
+ * reference reuses the previous query's cache count).  final_rows: the data
+ * rows of the array after the last compaction (*n_final = 0: no
+ * compaction).  Size q_* to the number of flag-2 ops and ent_* / final_rows
+ * to num + the number of flag-0 ops; every output array may be NULL. */
+int gts_update_plan(int num, const int *flags, const int *ids, int nops, int max_in_size,
+                    int *q_obj, int *q_time, int *q_cache, int *n_q,
+                    int *ent_src, int *ent_life, int *n_ent, int *final_rows, int *n_final);
 
 #ifdef __cplusplus
 }

@@ -26,10 +26,11 @@ def load_case(name):
 
 def sample_dir():
     """Directory holding the reference's sample data set, if present here:
-    the checkout, or the copy the oracle's reference build stages beside it
-    (oracle/_ref/sample, made by `make -C oracle ref`)."""
+    the copy the oracle's reference build stages (oracle/_ref/sample, made by
+    `make -C oracle ref`), or the checkout named by $GTS_REF_DIR."""
+    ref = os.environ.get("GTS_REF_DIR", "")
     for d in (os.environ.get("GTS_SAMPLE_DIR", ""), os.path.join(GOLDEN, "..", "..", "oracle", "_ref", "sample"),
-              "/root/reference/Datasets Sample"):
+              os.path.join(ref, "Datasets Sample") if ref else ""):
         if d and os.path.exists(os.path.join(d, "sbw_example.txt")):
             return d
     return None

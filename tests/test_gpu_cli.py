@@ -66,3 +66,29 @@ def test_cli_on_reference_sample(tmp_path):
         got = open(out).read().split("\n")[:3]
         want = open(os.path.join(GI.GOLDEN, gold)).read().split("\n")[:3]
         assert got == want, gold
+
+
+def test_reference_main_over_the_compat_headers(tmp_path):
+    """The reference's own src/main.cu, unmodified, compiled against
+    include/gts_ref (its entry points over this library; built by
+    `make -C oracle ref` where the checkout is) gives the reference's result
+    files on the reference's sample: kNN, range and the update stream."""
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                       "GTS_compat")
+    d = GI.sample_dir()
+    if d is None or not os.path.exists(exe):
+        pytest.skip("the reference's sample or its main.cu build over the compat headers is not present")
+    runs = [("0", "8", "sample_knn_k8.txt", "sbw_example_qid.txt"),
+            ("0", "20", "sample_knn_k20.txt", "sbw_example_qid.txt"),
+            ("1", "30", "sample_range_r30.txt", "sbw_example_qid.txt"),
+            ("2", "59", "sample_update_r59.txt", "sbw_example_u.txt")]
+    for op, par, gold, qf in runs:
+        out = tmp_path / gold
+        p = subprocess.run([exe, os.path.join(d, "sbw_example.txt"), os.path.join(d, qf), op, par, str(out)],
+                           capture_output=True, text=True, timeout=600)
+        assert p.returncode == 0, p.stderr
+        got = open(out).read().split("\n")
+        want = open(os.path.join(GI.GOLDEN, gold)).read().split("\n")
+        assert got[:3] == want[:3], gold
+        # the timing lines of main.cu's layout follow
+        assert got[3].startswith("Time of index construction: "), gold
