@@ -64,9 +64,9 @@ static int check_device()
 static int check_params(const gts_params *p)
 {
     if (p->tree_order < 2 || p->max_size < 1 || p->max_h < 1 || p->dis_code < 1 || p->infi_dis < 1 ||
-        p->max_in_size < 1) {
-        gts_set_error("invalid parameters (order %d, max_size %d, max_h %d)", p->tree_order, p->max_size,
-                      p->max_h);
+        p->max_in_size < 1 || !(p->mem_budget_gb >= 0.0)) {
+        gts_set_error("invalid parameters (order %d, max_size %d, max_h %d, mem_budget_gb %g)", p->tree_order,
+                      p->max_size, p->max_h, p->mem_budget_gb);
         return GTS_ERR_INVALID;
     }
     return GTS_OK;
@@ -256,8 +256,7 @@ static int build_common(int dim, int num, int metric, const float *rows, const c
         return GTS_ERR_INVALID;
     }
     *out = nullptr;
-    int rc = check_device();
-    if (rc) return rc;
+    int rc;
     gts_params p;
     if (params) p = *params; else gts_params_default(&p);
     if ((rc = check_params(&p))) return rc;
@@ -269,6 +268,7 @@ static int build_common(int dim, int num, int metric, const float *rows, const c
         gts_set_error("missing %s input", metric == 6 ? "string" : "row");
         return GTS_ERR_INVALID;
     }
+    if ((rc = check_device())) return rc;
     if (metric == 6 && kind == cudaMemcpyHostToDevice) {
         for (int i = 0; i < num; i++) {
             if (lens[i] < 0 || lens[i] > GTS_STR_STRIDE - 1) {

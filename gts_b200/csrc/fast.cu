@@ -68,6 +68,11 @@ constexpr long long kFWait = 1ll << 22;   // bounded mbarrier polls (each at mos
 constexpr float kEpsC = 5e-5f;        // q.c rows:  >= 2^-16 + 2 * 256 * 2^-24
 constexpr float kEpsR = 8e-5f;        // q.r rows:  >= 2^-16 + 2 * 256 * 2^-23 + 2^-23
 
+// The accumulation part grows with the products summed (2 kp of them), so
+// above kp = 128 both constants scale by kp / 128: at kp = 320,
+// 1.25e-4 >= 2^-16 + 2 * 640 * 2^-24 and 2e-4 >= 2^-16 + 2 * 640 * 2^-23 + 2^-23.
+__host__ __device__ __forceinline__ float eps_scale(int kp) { return kp <= 128 ? 1.f : (float)kp / 128.f; }
+
 // Record tail, after the BF16 operand rows (floats): w[128], dn[128], then
 // |c|, the valid-object count (int), max |bf16(r)|, max |w|, the radius
 // max |o - c| (rounded up).
@@ -286,9 +291,10 @@ __global__ void __launch_bounds__(128) k_fast_arec(const float *__restrict__ row
 // query's own block (the query is one of its objects), widened past every
 // rounding difference to the reference's value, lowers the query's bound.
 // The block's rows are read from the slot-ordered copy (one contiguous
-// 128 x kp range): one warp per 32 rows, lane l holding dimensions
-// 4l..4l+3, sixteen rows in flight per warp; warp 0 then takes out the
-// smallest value k - 1 times (four values per lane).
+// 128 x kp range): one warp per 32 rows, lane l holding the float4 columns
+// l, l + 32 and l + 64 (dimensions 4l.., 128 + 4l.., 256 + 4l.. up to kp),
+// sixteen rows in flight per warp; warp 0 then takes out the smallest value
+// k - 1 times (four values per lane).
 __global__ void __launch_bounds__(128) k_fast_seed(const float *__restrict__ rows, const int *__restrict__ qids,
                                                    FastSummary bs, int dim, int kp, int k, int *__restrict__ r2_bits)
 {
@@ -301,20 +307,31 @@ __global__ void __launch_bounds__(128) k_fast_seed(const float *__restrict__ row
     if (cnt < k) return;
     const unsigned vm = __ballot_sync(0xffffffffu, valid);   // this warp's 32 rows
     const float *qr = rows + (size_t)qid * dim;
-    const bool act = 4 * lane < kp;   // kp <= 128
-    float qv[4];
+    constexpr int kSeedCols = kFMaxKp / 128 + 1;   // float4 columns per lane (kp <= 320)
+    float qv[kSeedCols][4];
+    bool act[kSeedCols];
 #pragma unroll
-    for (int e = 0; e < 4; e++) qv[e] = (act && 4 * lane + e < dim) ? qr[4 * lane + e] : 0.f;
+    for (int c = 0; c < kSeedCols; c++) {
+        const int j0 = 4 * (lane + 32 * c);
+        act[c] = j0 < kp;
+#pragma unroll
+        for (int e = 0; e < 4; e++) qv[c][e] = (act[c] && j0 + e < dim) ? qr[j0 + e] : 0.f;
+    }
     const float *pb = bs.prow + (size_t)(base + warp * 32) * kp + 4 * lane;
 #pragma unroll
     for (int i0 = 0; i0 < 32; i0 += 16) {
         float acc[16];
 #pragma unroll
         for (int r = 0; r < 16; r++) {
-            float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (act && ((vm >> (i0 + r)) & 1u)) o = *reinterpret_cast<const float4 *>(pb + (size_t)(i0 + r) * kp);
-            const float e0 = o.x - qv[0], e1 = o.y - qv[1], e2 = o.z - qv[2], e3 = o.w - qv[3];
-            acc[r] = fmaf(e3, e3, fmaf(e2, e2, fmaf(e1, e1, e0 * e0)));
+            acc[r] = 0.f;
+            const bool rv = (vm >> (i0 + r)) & 1u;
+#pragma unroll
+            for (int c = 0; c < kSeedCols; c++) {
+                float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (act[c] && rv) o = *reinterpret_cast<const float4 *>(pb + (size_t)(i0 + r) * kp + 128 * c);
+                const float e0 = o.x - qv[c][0], e1 = o.y - qv[c][1], e2 = o.z - qv[c][2], e3 = o.w - qv[c][3];
+                acc[r] = fmaf(e3, e3, fmaf(e2, e2, fmaf(e1, e1, fmaf(e0, e0, acc[r]))));
+            }
         }
 #pragma unroll
         for (int r = 0; r < 16; r++) {
@@ -342,9 +359,9 @@ __global__ void __launch_bounds__(128) k_fast_seed(const float *__restrict__ row
             else x[3] = FLT_MAX;
         }
     }
-    // FP32 sum of at most 128 non-negative terms (4 per lane, then a 32-lane
-    // tree): relative error < 2^-19 against the reference's FP64 sum of the
-    // same FP32 differences
+    // FP32 sum of at most 320 non-negative terms (at most 12 per lane, then a
+    // 32-lane tree): relative error < 2^-19 against the reference's FP64 sum
+    // of the same FP32 differences
     if (lane == 0) atomicMin(&r2_bits[q], __float_as_int(mn * (1.f + 3e-5f)));
 }
 
@@ -378,31 +395,30 @@ __device__ __forceinline__ void need_load_tile(const float *__restrict__ qt, con
     for (int i = t; i < fs.kp * (kFT / 4); i += 256) dst[i] = src[i];
 }
 
+// Dimensions of the ball centres a pruning CTA holds at once: all of them up
+// to kp = 128, 64 at a time above (the tile's rows stay whole).
+__host__ __device__ __forceinline__ int need_kc(int kp) { return kp <= kFResKp ? kp : 64; }
+
+// Shared memory of a pruning CTA: the tile's rows [kp][128] and one chunk
+// of ball centres [need_kc][64] (FP32).
+__host__ __device__ __forceinline__ size_t need_smem_bytes(int kp)
+{
+    return sizeof(float) * ((size_t)kp * kFT + (size_t)need_kc(kp) * kFChunk);
+}
+
 // Balls c0 .. c0+63 (those below cend; with a list, balls list[0 .. cend-1]
 // and c0 = 0) against the tile: bit i of the result is set when some query
 // of the tile can reach ball i of the chunk within its seed:
 // |q - c|_lo - radius <= sqrt(seed).  256 threads: each computes
 // 8 queries (4tq..4tq+3 and 64+4tq..64+4tq+3, so a quarter warp reads 128
-// consecutive bytes: no bank conflicts) x 4 balls of FP32 q.c.
+// consecutive bytes: no bank conflicts) x 4 balls of FP32 q.c, over the
+// centre dimensions need_kc(kp) at a time.
 __device__ __forceinline__ uint64_t need_chunk(const float *__restrict__ cen, const float *__restrict__ c2, const float *__restrict__ rad,
                                int c0, int cend, const int *list, int kp, const float *Qs, float *Cs, NeedSmem &sm)
 {
     const int t = threadIdx.x;
+    const int kc = need_kc(kp);
     __syncthreads();   // previous chunk's Cs / flags consumed, list written
-    // thread (bb, j4): 4 dimensions of ball bb; consecutive threads take
-    // consecutive balls, so the shared-memory writes do not conflict
-    for (int i = t; i < (kp / 4) * kFChunk; i += 256) {
-        const int bb = i % kFChunk, j4 = i / kFChunk;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (c0 + bb < cend) {
-            const int ball = list ? list[bb] : c0 + bb;
-            v = *reinterpret_cast<const float4 *>(cen + (size_t)ball * kp + 4 * j4);
-        }
-        Cs[(4 * j4 + 0) * kFChunk + bb] = v.x;
-        Cs[(4 * j4 + 1) * kFChunk + bb] = v.y;
-        Cs[(4 * j4 + 2) * kFChunk + bb] = v.z;
-        Cs[(4 * j4 + 3) * kFChunk + bb] = v.w;
-    }
     if (t < kFChunk) {
         const bool ok = c0 + t < cend;
         const int ball = ok ? (list ? list[t] : c0 + t) : 0;
@@ -411,26 +427,43 @@ __device__ __forceinline__ uint64_t need_chunk(const float *__restrict__ cen, co
         sm.rads[t] = ok ? rad[ball] : -1.f;
     }
     if (t < 2) sm.flags[t] = 0u;
-    __syncthreads();
     const int tq = t & 15, tb = t >> 4;
     float acc[8][4];
 #pragma unroll
     for (int i = 0; i < 8; i++)
 #pragma unroll
         for (int c = 0; c < 4; c++) acc[i][c] = 0.f;
-    // kp is a multiple of 64: unrolled so the shared loads of later j are in
-    // flight while the FMAs of earlier ones run
+    for (int k0 = 0; k0 < kp; k0 += kc) {
+        if (k0 > 0) __syncthreads();   // the previous centre dimensions consumed
+        // thread (bb, j4): 4 dimensions of ball bb; consecutive threads take
+        // consecutive balls, so the shared-memory writes do not conflict
+        for (int i = t; i < (kc / 4) * kFChunk; i += 256) {
+            const int bb = i % kFChunk, j4 = i / kFChunk;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (c0 + bb < cend) {
+                const int ball = list ? list[bb] : c0 + bb;
+                v = *reinterpret_cast<const float4 *>(cen + (size_t)ball * kp + k0 + 4 * j4);
+            }
+            Cs[(4 * j4 + 0) * kFChunk + bb] = v.x;
+            Cs[(4 * j4 + 1) * kFChunk + bb] = v.y;
+            Cs[(4 * j4 + 2) * kFChunk + bb] = v.z;
+            Cs[(4 * j4 + 3) * kFChunk + bb] = v.w;
+        }
+        __syncthreads();
+        // kc is a multiple of 64: unrolled so the shared loads of later j are
+        // in flight while the FMAs of earlier ones run
 #pragma unroll 4
-    for (int j = 0; j < kp; j++) {
-        const float4 qa = *reinterpret_cast<const float4 *>(Qs + j * kFT + tq * 4);
-        const float4 qb = *reinterpret_cast<const float4 *>(Qs + j * kFT + 64 + tq * 4);
-        const float4 cc = *reinterpret_cast<const float4 *>(Cs + j * kFChunk + tb * 4);
-        const float qv[8] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
-        const float cv[4] = {cc.x, cc.y, cc.z, cc.w};
+        for (int j = 0; j < kc; j++) {
+            const float4 qa = *reinterpret_cast<const float4 *>(Qs + (k0 + j) * kFT + tq * 4);
+            const float4 qb = *reinterpret_cast<const float4 *>(Qs + (k0 + j) * kFT + 64 + tq * 4);
+            const float4 cc = *reinterpret_cast<const float4 *>(Cs + j * kFChunk + tb * 4);
+            const float qv[8] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
+            const float cv[4] = {cc.x, cc.y, cc.z, cc.w};
 #pragma unroll
-        for (int i = 0; i < 8; i++)
+            for (int i = 0; i < 8; i++)
 #pragma unroll
-            for (int c = 0; c < 4; c++) acc[i][c] = fmaf(qv[i], cv[c], acc[i][c]);
+                for (int c = 0; c < 4; c++) acc[i][c] = fmaf(qv[i], cv[c], acc[i][c]);
+        }
     }
     // FP32 dot of kp products: error <= kp 2^-23 |q||c|; the three-term
     // sum adds <= 4e-7 (|q|^2 + |c|^2)
@@ -592,10 +625,16 @@ struct FastTileArgs {
     // below r2lo are counted in rcnt[query] without a list entry
     float r2lo;
     int *rcnt;
+    int nsc;                     // streamed form: K-chunk stages
 };
 
 constexpr int kFS = 3;         // block stages, each with its own TMEM accumulator
 constexpr int kFAccCols = 160; // TMEM columns between accumulators (kFN = 144 used)
+// Streamed form (kp > kFResKp): K-chunk stages (a.nsc of them, at most
+// kFSCMax) and, per accumulator, the block's record tail in its own buffer.
+constexpr int kFSCMax = 4;
+constexpr uint32_t kFTailBytes = 1024u + 32u;   // w, dn, block scalars
+constexpr uint32_t kFTailPad = 1088u;
 
 // Candidates are staged in shared memory during an item; the capacity
 // (a.st_cap) is what the shared memory left after the operands holds.
@@ -605,6 +644,9 @@ struct __align__(16) FastCtl {
     uint64_t full[kFS];    // block copy landed
     uint64_t efree[kFS];   // epilogue of the block in this stage done (one arrive per epilogue warp)
     uint64_t mmad[kFS];    // MMA chain into TMEM accumulator s (one per stage) done
+    uint64_t tfull[kFS];   // streamed form: the block's record tail landed in tail buffer s
+    uint64_t cfull[kFSCMax];   // streamed form: K chunk landed in chunk stage c
+    uint64_t cfree[kFSCMax];   // streamed form: the MMAs reading chunk stage c done
     uint64_t afull;        // query tile copy landed
     uint32_t tmem;
     int tile, nblk;
@@ -649,7 +691,15 @@ constexpr uint32_t kStagedUnused = 0xffffffffu;
 // RANGE: range counts instead of kNN.  The bound stays the query's (r^2 with
 // the reference-arithmetic margin); objects certainly inside are counted per
 // thread, only the uncertain ones are listed; no bound heap.
-template <int CG, int KH, bool RANGE>
+//
+// KS (kp > kFResKp, where a whole record does not fit a stage beside the
+// query tile): the producer streams each block's operand rows in 64-wide K
+// chunks through a.nsc chunk stages -- a stage is refilled as soon as the
+// MMAs reading it are done (tcgen05.commit on cfree), one unit behind the
+// MMA issue -- and copies the block's record tail (w, dn, scalars) into the
+// tail buffer of its accumulator once the epilogue of the block three back
+// has freed both.  The epilogue is the same, reading the tail buffer.
+template <int CG, int KH, bool RANGE, bool KS>
 __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
 {
     constexpr int NT = 128 * CG;   // epilogue threads
@@ -663,7 +713,9 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
     const uint32_t arec_pad = (fs.arec_bytes + 1023u) & ~1023u;
     const uint32_t rec_pad = (fs.rec_bytes + 1023u) & ~1023u;
     unsigned char *B0 = base + arec_pad;
-    unsigned short *heap = reinterpret_cast<unsigned short *>(B0 + kFS * rec_pad);
+    // KS: chunk stages at B0 (1024-aligned), then the tail buffers
+    unsigned char *T0 = B0 + (KS ? (size_t)a.nsc * kFChunkBytes : 0);
+    unsigned short *heap = reinterpret_cast<unsigned short *>(KS ? T0 + kFS * kFTailPad : B0 + kFS * rec_pad);
     FastCtl &ctl = *reinterpret_cast<FastCtl *>(heap + (KH > 0 ? 0 : NT * a.k));
     FastStaged *stg = reinterpret_cast<FastStaged *>(&ctl + 1);
     const int st_cap = a.st_cap;
@@ -679,6 +731,11 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
             mbar_init(&ctl.efree[s], NEW);
         }
         for (int s = 0; s < kFS; s++) mbar_init(&ctl.mmad[s], 1);
+        for (int s = 0; s < kFS; s++) mbar_init(&ctl.tfull[s], 1);
+        for (int s = 0; s < kFSCMax; s++) {
+            mbar_init(&ctl.cfull[s], 1);
+            mbar_init(&ctl.cfree[s], 1);
+        }
         mbar_init(&ctl.afull, 1);
         ctl.err = 0;
         fence_mbar_init();
@@ -699,6 +756,9 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
     // whose MMA chain was committed, tile copies issued / waited
     long long c_iss = -1, c_wait = -1, m_iss = -1;
     int a_iss = 0, a_wait = 0;
+    // streamed form: K-chunk units run through the pipeline, last chunk copy
+    // issued / waited, last unit whose MMAs were committed, last tail issued
+    long long gunit = 0, u_iss = -1, u_wait = -1, u_mma = -1, t_iss = -1;
     unsigned long long blocks_done = 0, appended = 0;
 
     for (;;) {
@@ -724,7 +784,83 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
         if (tile < 0 || ctl.err) break;
         const int4 *tinfo = reinterpret_cast<const int4 *>(a.arec + (size_t)tile * fs.arec_bytes + 2 * fs.atile_bytes);
 
-        if (producer) {
+        if (producer && KS) {
+            if (lane == 0) {
+                const int nk = fs.nk, SC = a.nsc, total = nblk * nk;
+                auto issue_chunk = [&](int u) {   // unit u: chunk u % nk of the item's block u / nk
+                    const long long gu = gunit + u;
+                    const int s = (int)(gu % SC);
+                    const int blk = ctl.blk[u / nk];
+                    mbar_arrive_expect_tx(&ctl.cfull[s], (uint32_t)kFChunkBytes);
+                    bulk_g2s(B0 + (size_t)s * kFChunkBytes,
+                             a.recs + (size_t)blk * fs.rec_bytes + (size_t)(u % nk) * kFChunkBytes,
+                             (uint32_t)kFChunkBytes, &ctl.cfull[s]);
+                    u_iss = gu;
+                };
+                mbar_arrive_expect_tx(&ctl.afull, fs.arec_bytes);
+                bulk_g2s(base, a.arec + (size_t)tile * fs.arec_bytes, fs.arec_bytes, &ctl.afull);
+                a_iss++;
+                // chunk stages are free at an item start (the CTA synchronised
+                // after every MMA of the last item was consumed)
+                for (int u = 0; u < SC && u < total; u++) issue_chunk(u);
+                int err = 0;
+                if (!mbar_wait(&ctl.afull, (uint32_t)(a_wait & 1), kFWait)) err = 1;
+                else a_wait++;
+                const uint64_t dah = smem_desc_sw128(a_hi_s, 1024), dal = smem_desc_sw128(a_lo_s, 1024);
+                for (int j = 0; j < nblk && !err; j++) {
+                    const long long gi = gblk + j;
+                    const int acc = (int)(gi % kFS);
+                    const int blk = ctl.blk[j];
+                    // accumulator and tail buffer acc: free once the epilogue of
+                    // block gi - 3 is done
+                    if (gi >= kFS) {
+                        const long long gp = gi - kFS;
+                        if (!mbar_wait(&ctl.efree[acc], (uint32_t)((gp / kFS) & 1), kFWait)) { err = 3; break; }
+                    }
+                    mbar_arrive_expect_tx(&ctl.tfull[acc], kFTailBytes);
+                    bulk_g2s(T0 + (size_t)acc * kFTailPad, a.recs + (size_t)blk * fs.rec_bytes + fs.btile_bytes,
+                             kFTailBytes, &ctl.tfull[acc]);
+                    t_iss = gi;
+                    const uint32_t dt = tmem + (uint32_t)(acc * kFAccCols);
+                    for (int c = 0; c < nk; c++) {
+                        const int u = j * nk + c;
+                        const long long gu = gunit + u;
+                        const int s = (int)(gu % SC);
+                        if (!mbar_wait(&ctl.cfull[s], (uint32_t)((gu / SC) & 1), kFWait)) { err = 2; break; }
+                        u_wait = gu;
+                        tc_fence_after();
+                        const uint64_t db = smem_desc_sw128(smem_u32(B0 + (size_t)s * kFChunkBytes), 1024);
+#pragma unroll
+                        for (int kk = 0; kk < 4; kk++) {
+                            const uint64_t ao = ((uint64_t)c * (kFT * 128u) + (uint64_t)kk * 32u) >> 4;
+                            mma_bf16(dt, dah + ao, db + (((uint64_t)kk * 32u) >> 4), idesc, (c | kk) ? 1u : 0u);
+                        }
+#pragma unroll
+                        for (int kk = 0; kk < 4; kk++) {
+                            const uint64_t ao = ((uint64_t)c * (kFT * 128u) + (uint64_t)kk * 32u) >> 4;
+                            mma_bf16(dt, dal + ao, db + (((uint64_t)kk * 32u) >> 4), idesc, 1u);
+                        }
+                        mma_commit(&ctl.cfree[s]);
+                        u_mma = gu;
+                        // refill the previous unit's stage (its MMAs retire first)
+                        if (u >= 1 && u - 1 + SC < total) {
+                            const long long gp = gu - 1;
+                            if (!mbar_wait(&ctl.cfree[gp % SC], (uint32_t)((gp / SC) & 1), kFWait)) {
+                                err = 5;
+                                break;
+                            }
+                            issue_chunk(u - 1 + SC);
+                        }
+                    }
+                    if (err) break;
+                    mma_commit(&ctl.mmad[acc]);
+                    m_iss = gi;
+                }
+                if (err) atomicMax(&ctl.err, err);
+                blocks_done += nblk;
+            }
+            __syncwarp();
+        } else if (producer) {
             if (lane == 0) {
                 // block gi uses stage gi % 3 and TMEM accumulator gi % 3; its
                 // copy waits for the epilogue of block gi - 3 (which frees both)
@@ -789,7 +925,7 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
             const int4 inf = tinfo[lq];
             const int qi = inf.x;
             const float q2 = __int_as_float(inf.y), qn = __int_as_float(inf.z);
-            const float cr = 2.f * kEpsR * qn;
+            const float cr = 2.f * kEpsR * eps_scale(fs.kp) * qn;
             float hreg[KH > 0 ? KH : 1];
             if constexpr (KH > 0) {
 #pragma unroll
@@ -814,11 +950,12 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                     break;
                 }
                 tc_fence_after();
-                mbar_wait(&ctl.full[s], (uint32_t)((gi / kFS) & 1), kFWait);   // record tail visible here
+                // record tail visible here (KS: in the accumulator's tail buffer)
+                mbar_wait(KS ? &ctl.tfull[s] : &ctl.full[s], (uint32_t)((gi / kFS) & 1), kFWait);
                 // the bound the query's other column groups have reached
                 R2 = fminf(R2, __int_as_float(*(volatile const int *)&ctl.r2s[lq]));
-                const unsigned char *Bs = B0 + (size_t)s * rec_pad;
-                const float *tail = reinterpret_cast<const float *>(Bs + fs.btile_bytes);
+                const float *tail = reinterpret_cast<const float *>(
+                    KS ? T0 + (size_t)s * kFTailPad : B0 + (size_t)s * rec_pad + fs.btile_bytes);
                 const float *wv = tail + kTailW, *dn = tail + kTailDn;
                 const float cn = tail[kTailC], rb = tail[kTailRb], wb = tail[kTailWb], brad = tail[kTailRad];
                 const uint32_t taddr = tmem + trow + (uint32_t)(s * kFAccCols);
@@ -832,7 +969,7 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                 tmem_ld4_nowait(taddr + 128, cv);
                 tmem_wait_ld(cv);
                 const float qc = __uint_as_float(cv[0]) + __uint_as_float(cv[1]) + __uint_as_float(cv[2]);
-                const float ec = 2.f * kEpsC * qn * cn + 1e-6f;
+                const float ec = 2.f * kEpsC * eps_scale(fs.kp) * qn * cn + 1e-6f;
                 const float c2 = cn * cn;
                 const float qmc2 = q2 - 2.f * qc + c2;
                 const float A = 2.000004f * sqrtf(fmaxf(qmc2 + ec + 4e-6f * (q2 + c2), 0.f)) + 2e-6f * cn;
@@ -969,6 +1106,7 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
             if (RANGE && qi >= 0 && certain) atomicAdd(a.rcnt + qi, certain);
         }
         gblk += nblk;
+        if (KS) gunit += (long long)nblk * fs.nk;
         tc_fence_before();
         __syncthreads();   // item done: every MMA consumed, stages and A free
         tc_fence_after();
@@ -1000,6 +1138,14 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
             mbar_wait(&ctl.full[gi % kFS], (uint32_t)((gi / kFS) & 1), kFWait);
         if (a_wait < a_iss) mbar_wait(&ctl.afull, (uint32_t)((a_iss - 1) & 1), kFWait);
         if (m_iss >= 0) mbar_wait(&ctl.mmad[m_iss % kFS], (uint32_t)((m_iss / kFS) & 1), kFWait);
+        if (KS) {
+            const int SC = a.nsc;
+            for (long long gu = u_wait + 1; gu <= u_iss; gu++)
+                mbar_wait(&ctl.cfull[gu % SC], (uint32_t)((gu / SC) & 1), kFWait);
+            if (u_mma >= 0) mbar_wait(&ctl.cfree[u_mma % SC], (uint32_t)((u_mma / SC) & 1), kFWait);
+            for (long long gi = t_iss - kFS + 1 > 0 ? t_iss - kFS + 1 : 0; gi <= t_iss; gi++)
+                mbar_wait(&ctl.tfull[gi % kFS], (uint32_t)((gi / kFS) & 1), kFWait);
+        }
     }
     if (a.stats && appended) atomicAdd(&a.stats[5], appended);
     if (a.stats && producer && lane == 0 && blocks_done) {
@@ -1028,6 +1174,10 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
 // side, each in the sequential order.
 constexpr int kFinB = 16;
 
+// KPM: the widest row the term buffer holds (kFResKp or kFMaxKp); FINB
+// candidates per batch (the buffer, FINB x (KPM + 1) doubles, stays within
+// the static shared memory).
+template <int KPM, int FINB>
 __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ rows, int dim, int num,
                                                     const float *__restrict__ prow, int kp,
                                                     const int *__restrict__ ids_of_slot, int nslots,
@@ -1046,10 +1196,10 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
     // the upper bounds (dead once the bound is set) share their space with the
     // pow terms; +1 double per row: lane c's reads of column j miss each
     // other's banks
-    constexpr int kTermsBytes = kFinB * (kFMaxKp + 1) * 8;
+    constexpr int kTermsBytes = FINB * (KPM + 1) * 8;
     __shared__ __align__(16) unsigned char scratch[kTermsBytes > 4 * kFCand ? kTermsBytes : 4 * kFCand];
     float *ubs = reinterpret_cast<float *>(scratch);
-    double(*terms)[kFMaxKp + 1] = reinterpret_cast<double(*)[kFMaxKp + 1]>(scratch);
+    double(*terms)[KPM + 1] = reinterpret_cast<double(*)[KPM + 1]>(scratch);
     __shared__ int ns;
     __shared__ float kub;
     const int q = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -1126,8 +1276,8 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
     const double lim = (double)R2 * (1.0 - 1e-6);
     // Pass 0 sums exact squares e * e (a float difference squared
     // is exact in FP64) instead of pow(e, 2).  pow is within 2 ulp of the
-    // square, so over dim <= 128 terms the sequential sums differ by less
-    // than 2.9e-14 relative and the distances by less than 1.6e-14; with the
+    // square, so over dim <= 320 terms the sequential sums differ by less
+    // than 7.2e-14 relative and the distances by less than 3.6e-14; with the
     // margin delta = 1e-13 v the pass-0 values give the reference's float
     // values, order and bound tests unless some value lies within delta of a
     // float rounding midpoint, of another candidate's value or of the bound.
@@ -1138,8 +1288,8 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
     int p2 = 1;
     while (p2 < n) p2 <<= 1;
     for (int pass = 0; pass < 2; pass++) {
-        for (int b0 = 0; b0 < n; b0 += kFinB) {
-            const int nb = min(kFinB, n - b0);
+        for (int b0 = 0; b0 < n; b0 += FINB) {
+            const int nb = min(FINB, n - b0);
             for (int c = warp; c < nb; c += 4) {
                 const float *orow = prow + (size_t)cl[b0 + c] * kp;
                 if (pass == 0) {
@@ -1324,24 +1474,71 @@ struct FastCfg {
 static int cfg_pack(const FastCfg &c) { return 1 | (c.learned ? 2 : 0) | (c.cg << 2) | (c.item << 8); }
 static FastCfg cfg_unpack(int v) { return FastCfg{(v & 2) != 0, (v >> 2) & 7, (v >> 8) & 63}; }
 
+static bool fast_tile_fits(const FastShape &fs, int cg, int k);
+
 static FastCfg fast_default_cfg(const gts_index *idx, int k)
 {
     // measured on clustered data: the own-block seed is tight for small k,
-    // the learned radius pays for its re-answers from k = 16 on
-    return FastCfg{idx->mlp_ready && k >= 16, fast_cg(k), 16};
+    // the learned radius pays for its re-answers from k = 16 on; the column
+    // groups are the most whose shared memory fits this dimension
+    int cg = fast_cg(k);
+    while (cg > 1 && !fast_tile_fits(fast_shape(idx->dim), cg, k)) cg >>= 1;
+    return FastCfg{idx->mlp_ready && k >= 16, cg, 16};
 }
 
-template <int CG, int KH, bool RANGE = false>
+// Shared memory of the filter kernel before candidate staging: the query
+// tile, the block stages (whole records, or for kp > kFResKp nsc K-chunk
+// stages and three tail buffers), the bound heaps (k > 16) and the control
+// block.  nsc = 0 for the resident form.
+static size_t fast_tile_fixed_smem(const FastShape &fs, int cg, int k, bool heap_in_smem, int nsc)
+{
+    const uint32_t arec_pad = (fs.arec_bytes + 1023u) & ~1023u;
+    const uint32_t rec_pad = (fs.rec_bytes + 1023u) & ~1023u;
+    const size_t heap = heap_in_smem ? sizeof(unsigned short) * 128 * cg * (size_t)k : 0;
+    const size_t stages = fs.kp > kFResKp ? (size_t)nsc * kFChunkBytes + kFS * (size_t)kFTailPad
+                                          : kFS * (size_t)rec_pad;
+    return 1024 + (size_t)arec_pad + stages + heap + sizeof(FastCtl) + 64;
+}
+
+static int smem_optin()
+{
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return optin;
+}
+
+// K-chunk stages of the streamed form that fit beside at least 4 KB of
+// candidate staging (at most kFSCMax); 0 when not even two fit.
+static int fast_tile_stages(const FastShape &fs, int cg, int k, bool heap_in_smem)
+{
+    const size_t optin = (size_t)smem_optin();
+    for (int nsc = kFSCMax; nsc >= 2; nsc--)
+        if (fast_tile_fixed_smem(fs, cg, k, heap_in_smem, nsc) + 4096 <= optin) return nsc;
+    return 0;
+}
+
+// The filter configuration (column groups cg, bound heap in shared memory
+// for k > 16) fits this index's shared-memory plan.
+static bool fast_tile_fits(const FastShape &fs, int cg, int k)
+{
+    const bool heap = k > 16;
+    if (fs.kp > kFResKp) return fast_tile_stages(fs, cg, k, heap) >= 2;
+    return fast_tile_fixed_smem(fs, cg, k, heap, 0) + 32 * sizeof(FastStaged) <= (size_t)smem_optin();
+}
+
+template <int CG, int KH, bool RANGE = false, bool KS = false>
 static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
 {
-    const uint32_t arec_pad = (a.fs.arec_bytes + 1023u) & ~1023u;
-    const uint32_t rec_pad = (a.fs.rec_bytes + 1023u) & ~1023u;
-    const size_t heap = KH > 0 ? 0 : sizeof(unsigned short) * 128 * CG * (size_t)a.k;
-    const size_t fixed = 1024 + (size_t)arec_pad + kFS * (size_t)rec_pad + heap + sizeof(FastCtl) + 64;
-    int dev = 0, optin = 0;
-    GTS_CUDA_TRY(cudaGetDevice(&dev));
-    GTS_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     FastTileArgs b = a;
+    b.nsc = KS ? fast_tile_stages(a.fs, CG, a.k, KH == 0) : 0;
+    if (KS && b.nsc < 2) {
+        gts_set_error("tensor-core filter: kp %d leaves no room for two K-chunk stages (%d column groups, k %d)",
+                      a.fs.kp, CG, a.k);
+        return GTS_ERR_INVALID;
+    }
+    const size_t fixed = fast_tile_fixed_smem(a.fs, CG, a.k, KH == 0, b.nsc);
+    const int optin = smem_optin();
     b.st_cap = (int)std::min<size_t>(kFStageMax, optin > (int)fixed ? ((size_t)optin - fixed) / sizeof(FastStaged) : 0);
     b.st_cap &= ~31;
     if (b.st_cap < 32) {
@@ -1349,11 +1546,18 @@ static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
         return GTS_ERR_INVALID;
     }
     const size_t smem = fixed + sizeof(FastStaged) * (size_t)b.st_cap;
-    GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_tile<CG, KH, RANGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_tile<CG, KH, RANGE, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
-    k_fast_tile<CG, KH, RANGE><<<grid, 128 * CG + 32, smem, st>>>(b);
+    k_fast_tile<CG, KH, RANGE, KS><<<grid, 128 * CG + 32, smem, st>>>(b);
     GTS_CUDA_TRY(cudaGetLastError());
     return GTS_OK;
+}
+
+template <int CG, int KH, bool RANGE = false>
+static int launch_fast_tile_ks(const FastTileArgs &a, int grid, cudaStream_t st)
+{
+    return a.fs.kp > kFResKp ? launch_fast_tile_cg<CG, KH, RANGE, true>(a, grid, st)
+                             : launch_fast_tile_cg<CG, KH, RANGE, false>(a, grid, st);
 }
 
 static int launch_fast_tile(const FastTileArgs &a, int cg, int grid, cudaStream_t st)
@@ -1361,22 +1565,22 @@ static int launch_fast_tile(const FastTileArgs &a, int cg, int grid, cudaStream_
     // k <= 16: the k kept bounds live in registers
     if (a.k <= 8) {
         switch (cg) {
-        case 4: return launch_fast_tile_cg<4, 8>(a, grid, st);
-        case 2: return launch_fast_tile_cg<2, 8>(a, grid, st);
-        default: return launch_fast_tile_cg<1, 8>(a, grid, st);
+        case 4: return launch_fast_tile_ks<4, 8>(a, grid, st);
+        case 2: return launch_fast_tile_ks<2, 8>(a, grid, st);
+        default: return launch_fast_tile_ks<1, 8>(a, grid, st);
         }
     }
     if (a.k <= 16) {
         switch (cg) {
-        case 4: return launch_fast_tile_cg<4, 16>(a, grid, st);
-        case 2: return launch_fast_tile_cg<2, 16>(a, grid, st);
-        default: return launch_fast_tile_cg<1, 16>(a, grid, st);
+        case 4: return launch_fast_tile_ks<4, 16>(a, grid, st);
+        case 2: return launch_fast_tile_ks<2, 16>(a, grid, st);
+        default: return launch_fast_tile_ks<1, 16>(a, grid, st);
         }
     }
     switch (cg) {
-    case 4: return launch_fast_tile_cg<4, 0>(a, grid, st);
-    case 2: return launch_fast_tile_cg<2, 0>(a, grid, st);
-    default: return launch_fast_tile_cg<1, 0>(a, grid, st);
+    case 4: return launch_fast_tile_ks<4, 0>(a, grid, st);
+    case 2: return launch_fast_tile_ks<2, 0>(a, grid, st);
+    default: return launch_fast_tile_ks<1, 0>(a, grid, st);
     }
 }
 
@@ -1528,7 +1732,7 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
         GTS_CUDA_TRY(cudaEventRecord(idx->side_ev[1], ss));
         GTS_CUDA_TRY(cudaStreamWaitEvent(st, idx->side_ev[1], 0));
     }
-    const size_t need_smem = sizeof(float) * (size_t)fs.kp * (kFT + kFChunk);
+    const size_t need_smem = need_smem_bytes(fs.kp);
     GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_sb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
     GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
     k_need_sb<<<dim3(ntiles, (nsb + kFChunk - 1) / kFChunk), 256, need_smem, st>>>(
@@ -1574,9 +1778,16 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
         GTS_CUDA_TRY(cudaEventRecordWithFlags(idx->fev[1], st, capturing ? cudaEventRecordExternal : 0));
     k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 1ull);
     idx->kernel_launches++;
-    k_fast_final<<<qnum, 128, 0, st>>>(idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k,
-                                        idx->params.infi_dis, r.cpos, r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids,
-                                        d_dists, d_fail, r.ctr, idx->d_stats);
+    if (fs.kp <= kFResKp)
+        k_fast_final<kFResKp, kFinB><<<qnum, 128, 0, st>>>(idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids,
+                                                          nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos, r.clb,
+                                                          r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr,
+                                                          idx->d_stats);
+    else
+        k_fast_final<kFMaxKp, kFinB / 2><<<qnum, 128, 0, st>>>(idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids,
+                                                              nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
+                                                              r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists,
+                                                              d_fail, r.ctr, idx->d_stats);
     idx->kernel_launches++;
     GTS_CUDA_TRY(cudaGetLastError());
     return GTS_OK;
@@ -1832,6 +2043,7 @@ static int fast_autotune(gts_index *idx, FastCall &fc, int qc, const int *d_qids
     for (int learned = 0; learned <= (idx->mlp_ready ? 1 : 0) && rc == GTS_OK; learned++)
         for (int cg = 4; cg >= 1 && rc == GTS_OK; cg >>= 1) {
             if (k > 16 && cg * k > 128) continue;   // heaps: 128 cg threads x k x 2 bytes <= 32 KB
+            if (!fast_tile_fits(fast_shape(idx->dim), cg, k)) continue;
             for (int item = 8; item <= kFItemMax && rc == GTS_OK; item *= 2) {
                 const FastCfg c{learned != 0, cg, item};
                 if ((rc = (int)cudaEventRecord(e0, st)) != 0) {
@@ -1870,16 +2082,39 @@ int fast_prepare_now(gts_index *idx, cudaStream_t st, int *done)
     return rc;
 }
 
+// Queries per filter run: at most kFMaxBatch, halved (in whole tiles) until
+// the scratch of one run, per_run(q) bytes, fits the call's budget; a run of
+// one tile that does not fit is an error.
+template <typename F>
+static int run_queries_for_budget(const gts_index *idx, int qnum, F per_run, int *qc)
+{
+    const size_t budget = search_budget(idx);
+    int q = std::min(qnum, kFMaxBatch);
+    while (q > kFT && per_run(q) > budget) q = std::max(kFT, (q / 2 + kFT - 1) / kFT * kFT);
+    if (per_run(q) > budget) {
+        gts_set_error("scratch budget of %zu bytes is below the %zu bytes of one %d-query filter run", budget,
+                      per_run(q), q);
+        return GTS_ERR_NOMEM;
+    }
+    *qc = q;
+    return GTS_OK;
+}
+
 int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                     float *d_dists, cudaStream_t st)
 {
     int rc = fast_prepare(idx, st);
     if (rc) return rc;
-    // one scratch region for a batch of at most kFMaxBatch queries, reused
-    // by the re-answer stages, plus their bookkeeping
-    const int qc = std::min(qnum, kFMaxBatch);
-    const size_t rbytes = (plan_run(idx, qc, nullptr, nullptr) + 255) & ~(size_t)255;
-    const size_t bbytes = (plan_book(qc, k, nullptr, nullptr) + 255) & ~(size_t)255;
+    // one scratch region for a run of at most kFMaxBatch queries (fewer when
+    // the call's budget is smaller), reused by the re-answer stages, plus
+    // their bookkeeping
+    auto rbytes_of = [&](int q) { return (plan_run(idx, q, nullptr, nullptr) + 255) & ~(size_t)255; };
+    auto bbytes_of = [&](int q) { return (plan_book(q, k, nullptr, nullptr) + 255) & ~(size_t)255; };
+    int qc = 0;
+    if ((rc = run_queries_for_budget(idx, qnum, [&](int q) { return rbytes_of(q) + 3 * bbytes_of(q); }, &qc)))
+        return rc;
+    const size_t rbytes = rbytes_of(qc);
+    const size_t bbytes = bbytes_of(qc);
     if ((rc = ensure_scratch(idx, rbytes + 3 * bbytes))) return rc;
     FastCall fc;
     fc.region = (unsigned char *)idx->scratch;
@@ -1905,12 +2140,13 @@ int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d
 int search_knn_fast_fixed(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                           float *d_dists, unsigned char *scratch, size_t bytes, cudaStream_t st)
 {
-    if (!fast_supported(idx, k)) {
-        gts_set_error("fixed-scratch kNN supports the L2 metric with dim <= %d and 1 <= k <= %d", kFMaxKp, kFMaxK);
+    if (!fast_supported(idx, k) || idx->dim > kFResKp) {
+        gts_set_error("fixed-scratch kNN supports the L2 metric with dim <= %d and 1 <= k <= %d", kFResKp, kFMaxK);
         return GTS_ERR_INVALID;
     }
     if (!idx->fast_recs) {
-        gts_set_error("the index has no filter records yet: one GTS_FORM_FAST kNN call on it must come first");
+        gts_set_error("the index has no filter records (none built yet, or a rebuild or update dropped them): one "
+                      "GTS_FORM_FAST kNN call or gts_index_prepare on it must come first");
         return GTS_ERR_INVALID;
     }
     if (qnum <= 0) return GTS_OK;
@@ -2045,9 +2281,13 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
     if (rc) return rc;
     const FastShape fs = fast_shape(idx->dim);
     const int nb = idx->fast_nb, nsb = idx->fast_nsb, nsbw = (nsb + 31) / 32;
-    const int qc = std::min(qnum, kFMaxBatch);
-    const size_t rbytes = (plan_run(idx, qc, nullptr, nullptr) + 255) & ~(size_t)255;
-    const size_t ib = ((size_t)qc * sizeof(int) + 255) & ~(size_t)255;
+    auto rbytes_of = [&](int q) { return (plan_run(idx, q, nullptr, nullptr) + 255) & ~(size_t)255; };
+    auto ib_of = [&](int q) { return ((size_t)q * sizeof(int) + 255) & ~(size_t)255; };
+    int qc = 0;
+    if ((rc = run_queries_for_budget(idx, qnum, [&](int q) { return rbytes_of(q) + 4 * ib_of(q); }, &qc)))
+        return rc;
+    const size_t rbytes = rbytes_of(qc);
+    const size_t ib = ib_of(qc);
     if ((rc = ensure_scratch(idx, rbytes + 4 * ib))) return rc;
     unsigned char *region = (unsigned char *)idx->scratch;
     int *rcnt = (int *)(region + rbytes), *fail = (int *)(region + rbytes + ib);
@@ -2081,7 +2321,7 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
         GTS_CUDA_TRY(cudaMemsetAsync(rb.ctr, 0, 8 * sizeof(int), st));
         GTS_CUDA_TRY(cudaMemsetAsync(rb.bcnt, 0, sizeof(int) * ntiles, st));
         k_fast_arec<<<ntiles, 128, 0, st>>>(idx->rows, dq, rb.order, n, idx->dim, fs, rb.arec, rb.qt);
-        const size_t need_smem = sizeof(float) * (size_t)fs.kp * (kFT + kFChunk);
+        const size_t need_smem = need_smem_bytes(fs.kp);
         GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_sb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
         GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
         k_need_sb<<<dim3(ntiles, (nsb + kFChunk - 1) / kFChunk), 256, need_smem, st>>>(
@@ -2114,7 +2354,7 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
         a.rcnt = rcnt;
         const bool timed = idx->time_filter && idx->fev[0];
         if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[0], st));
-        if ((rc = launch_fast_tile_cg<4, 8, true>(a, nsm, st))) return rc;
+        if ((rc = launch_fast_tile_ks<4, 8, true>(a, nsm, st))) return rc;
         if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[1], st));
         k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 1ull);
         k_fast_range_final<<<n, 128, 0, st>>>(idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, dq, r,
@@ -2183,6 +2423,12 @@ extern "C" int gts_fast_config_set(gts_index *idx, int k, int learned, int col_g
         col_groups * k > 128 || (item_blocks != 8 && item_blocks != 16 && item_blocks != 32)) {
         gts_set_error("gts_fast_config_set: k in [1, 64], column groups 1/2/4 with groups * k <= 128, "
                       "8/16/32 blocks per item");
+        return GTS_ERR_INVALID;
+    }
+    if (idx->metric == gts::kL2 && idx->dim <= gts::kFMaxKp &&
+        !gts::fast_tile_fits(gts::fast_shape(idx->dim), col_groups, k)) {
+        gts_set_error("gts_fast_config_set: %d column groups at k %d do not fit the shared memory at dim %d",
+                      col_groups, k, idx->dim);
         return GTS_ERR_INVALID;
     }
     idx->fast_cfg[k] = gts::cfg_pack(gts::FastCfg{learned != 0, col_groups, item_blocks});

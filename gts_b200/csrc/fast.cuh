@@ -13,7 +13,10 @@ namespace gts {
 constexpr int kFB = 128;              // slots per block
 constexpr int kFN = 144;              // B rows per block: objects + centre rows + padding
 constexpr int kFT = 128;              // queries per tile (A rows, TMEM lanes)
-constexpr int kFMaxKp = 128;          // padded dimension limit of this path (shared-memory budget)
+constexpr int kFMaxKp = 320;          // padded dimension limit of this path
+constexpr int kFResKp = 128;          // up to this padded dimension a block record sits whole in one
+                                      // filter stage; above it the filter streams K in 64-wide chunks
+constexpr int kFChunkBytes = kFN * 128;   // one 64-wide K chunk of a block's operand rows
 constexpr int kFMaxK = 64;
 
 // Block order (hierarchical k-means, fast_order.cu):

@@ -102,6 +102,7 @@ __global__ void k_o_seed(int nseg, int dim, const float *__restrict__ rows, cons
 // its sum and count.  Pass 1 (final): the sort key (segment << 32 | child)
 // for k-means segments, (segment << 32 | projection on c1 - c0) for halving
 // segments, (segment << 32) for leaves; counts of the k-means children.
+template <int NX>
 __global__ void __launch_bounds__(256) k_o_assign(int n, int dim, const float *__restrict__ rows,
                                                   const int *__restrict__ perm, const int *__restrict__ sid,
                                                   const int *__restrict__ kind, const int *__restrict__ kk,
@@ -109,7 +110,7 @@ __global__ void __launch_bounds__(256) k_o_assign(int n, int dim, const float *_
                                                   float *__restrict__ csum, int *__restrict__ ccnt, int final_pass,
                                                   unsigned long long *__restrict__ keys)
 {
-    __shared__ float ssum[kOrdBranch * kFMaxKp];
+    __shared__ float ssum[kOrdBranch * NX * 32];
     __shared__ int scnt[kOrdBranch];
     const int p0 = blockIdx.x * kOAsgPos, p1 = min(n, p0 + kOAsgPos);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -128,9 +129,9 @@ __global__ void __launch_bounds__(256) k_o_assign(int n, int dim, const float *_
             continue;
         }
         const float *xr = rows + (size_t)perm[pos] * dim;
-        float x[kFMaxKp / 32];
+        float x[NX];
 #pragma unroll
-        for (int i = 0; i < kFMaxKp / 32; i++) {
+        for (int i = 0; i < NX; i++) {
             const int d = lane + 32 * i;
             x[i] = d < dim ? xr[d] : 0.f;
         }
@@ -141,7 +142,7 @@ __global__ void __launch_bounds__(256) k_o_assign(int n, int dim, const float *_
             const float *c = cent + (size_t)(cb + j) * dim;
             float acc = 0.f;
 #pragma unroll
-            for (int i = 0; i < kFMaxKp / 32; i++) {
+            for (int i = 0; i < NX; i++) {
                 const int d = lane + 32 * i;
                 if (d < dim) {
                     const float e = x[i] - c[d];
@@ -157,14 +158,14 @@ __global__ void __launch_bounds__(256) k_o_assign(int n, int dim, const float *_
         if (!final_pass) {
             if (uni) {
 #pragma unroll
-                for (int i = 0; i < kFMaxKp / 32; i++) {
+                for (int i = 0; i < NX; i++) {
                     const int d = lane + 32 * i;
                     if (d < dim) atomicAdd(&ssum[bj * dim + d], x[i]);
                 }
                 if (lane == 0) atomicAdd(&scnt[bj], 1);
             } else {
 #pragma unroll
-                for (int i = 0; i < kFMaxKp / 32; i++) {
+                for (int i = 0; i < NX; i++) {
                     const int d = lane + 32 * i;
                     if (d < dim) atomicAdd(&csum[(size_t)(cb + bj) * dim + d], x[i]);
                 }
@@ -179,7 +180,7 @@ __global__ void __launch_bounds__(256) k_o_assign(int n, int dim, const float *_
                 const float *c0 = cent + (size_t)cb * dim, *c1 = c0 + dim;
                 float p = 0.f;
 #pragma unroll
-                for (int i = 0; i < kFMaxKp / 32; i++) {
+                for (int i = 0; i < NX; i++) {
                     const int d = lane + 32 * i;
                     if (d < dim) p = fmaf(x[i], c1[d] - c0[d], p);
                 }
@@ -368,12 +369,21 @@ int fast_block_order(gts_index *idx, FastOrder *out, cudaStream_t st)
         for (int it = 0; it < kOrdIters; it++) {
             GTS_CUDA_TRY(cudaMemsetAsync(csum, 0, sizeof(float) * (size_t)C * dim, st));
             GTS_CUDA_TRY(cudaMemsetAsync(ccnt, 0, sizeof(int) * (size_t)C, st));
-            k_o_assign<<<agrid, 256, 0, st>>>(n, dim, idx->rows, perm, sid, kind, kk, cbase, cent, csum, ccnt, 0,
-                                              keys);
+            if (dim <= kFResKp)
+                k_o_assign<kFResKp / 32><<<agrid, 256, 0, st>>>(n, dim, idx->rows, perm, sid, kind, kk, cbase, cent,
+                                                               csum, ccnt, 0, keys);
+            else
+                k_o_assign<kFMaxKp / 32><<<agrid, 256, 0, st>>>(n, dim, idx->rows, perm, sid, kind, kk, cbase, cent,
+                                                               csum, ccnt, 0, keys);
             k_o_update<<<ugrid, 256, 0, st>>>(C, dim, csum, ccnt, cent);
         }
         GTS_CUDA_TRY(cudaMemsetAsync(ccnt, 0, sizeof(int) * (size_t)C, st));
-        k_o_assign<<<agrid, 256, 0, st>>>(n, dim, idx->rows, perm, sid, kind, kk, cbase, cent, csum, ccnt, 1, keys);
+        if (dim <= kFResKp)
+            k_o_assign<kFResKp / 32><<<agrid, 256, 0, st>>>(n, dim, idx->rows, perm, sid, kind, kk, cbase, cent, csum,
+                                                           ccnt, 1, keys);
+        else
+            k_o_assign<kFMaxKp / 32><<<agrid, 256, 0, st>>>(n, dim, idx->rows, perm, sid, kind, kk, cbase, cent, csum,
+                                                           ccnt, 1, keys);
         int sbits = 1;
         while ((1 << sbits) < nseg) sbits++;
         size_t tb3 = cub_bytes;

@@ -113,6 +113,15 @@ int search_range_ids(gts_index *idx, const int *d_qids, int qnum, float r, int *
 template <typename T>
 int dev_alloc(T **p, size_t n, size_t *acct);
 
+// Device scratch one search call may hold (gts_params.mem_budget_gb; 0 means
+// 8 GiB).  The fast form sizes its runs of queries, the seeded plain form its
+// chunks and the update path its query batches to fit it.
+inline size_t search_budget(const gts_index *idx)
+{
+    const double gb = idx->params.mem_budget_gb;
+    return gb > 0 ? (size_t)(gb * 1073741824.0) : ((size_t)8 << 30);
+}
+
 // Grow idx->scratch to at least `bytes`.
 int ensure_scratch(gts_index *idx, size_t bytes);
 // Grow idx->io to at least `bytes`.

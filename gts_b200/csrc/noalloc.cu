@@ -14,43 +14,36 @@
 // on it; calls on one stream, or ordered by events, are safe.  Nothing in the
 // array has to start at zero: each call clears the counters it uses (work
 // item counter, candidate counts, failure count) on its stream before use.
-// The first call on a device looks the array up with cudaGetSymbolAddress,
-// which loads this file's module; that first call should come before any
-// stream capture.
-#include <mutex>
+// Every call looks the array up with cudaGetSymbolAddress on the current
+// device (cheap once the module is loaded), so a context that was reset and
+// made again gets the new address; the first call on a device loads this
+// file's module and should come before any stream capture.
+//
+// Index size: the fixed array also holds one run's per-tile block lists
+// (4 bytes per filter block per tile) and work items, next to the 1,024-slot
+// candidate lists of the queries (about 6.3 MiB at 512 queries).  Past about
+// 35 million objects (some 270,000 filter blocks) those no longer fit beside
+// 512 queries and a call fails with "fixed scratch ... too small"; fewer
+// queries per call fit larger indexes.
 #include "index.cuh"
 
 namespace {
 
 constexpr int kNoAllocMaxQueries = 512;
 constexpr size_t kNoAllocBytes = (size_t)12 << 20;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-std::mutex g_noalloc_mu;
-unsigned char *g_noalloc_ptr[kMaxDevices] = {};
-
-// Device address of the array on the current device, looked up once.
+// Device address of the array on the current device.
 int noalloc_scratch(unsigned char **out)
 {
-    int dev = 0;
-    GTS_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) {
-        gts_set_error("gts_knn_device_noalloc: device %d beyond the %d supported", dev, kMaxDevices);
-        return GTS_ERR_INVALID;
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        gts_set_error("gts_knn_device_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+        return GTS_ERR_CUDA;
     }
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            gts_set_error("gts_knn_device_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-            return GTS_ERR_CUDA;
-        }
-        g_noalloc_ptr[dev] = (unsigned char *)p;
-    }
-    *out = g_noalloc_ptr[dev];
+    *out = (unsigned char *)p;
     return GTS_OK;
 }
 

@@ -806,18 +806,63 @@ __global__ void k_scatter_q(const int *idx, int n, int k, const float *kth_s, co
     }
 }
 
+// Scratch of one seeded chunk of qn queries (offsets in the handle's region).
+struct LearnedPlan {
+    size_t seed, fail, n, q, kth, ids, dis, end;
+};
+
+static LearnedPlan plan_learned(int qn, int k)
+{
+    LearnedPlan p;
+    size_t off = 0;
+    auto take = [&](size_t b) { size_t o = off; off += (b + 255) & ~(size_t)255; return o; };
+    p.seed = take(4 * (size_t)qn);
+    p.fail = take(4 * (size_t)qn);
+    p.n = take(16);
+    p.q = take(4 * (size_t)qn);
+    p.kth = take(4 * (size_t)qn);
+    p.ids = take(4 * (size_t)qn * k);
+    p.dis = take(4 * (size_t)qn * k);
+    p.end = off;
+    return p;
+}
+
+static int search_knn_plain_learned_chunk(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth,
+                                          int *d_ids, float *d_dists, cudaStream_t st);
+
 // The plain traversal seeded by the learned radius (GTS_FORM_PLAIN_LEARNED):
 // every query starts pruning from its predicted k-th distance instead of
 // from infinity; queries whose radius held fewer than k objects are answered
 // again by the unseeded traversal, so the results are the plain form's.
+// Queries run in chunks whose scratch fits the call's budget.
 int search_knn_plain_learned(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                              float *d_dists, cudaStream_t st)
 {
-    size_t off = 0;
-    auto take = [&](size_t b) { size_t o = off; off += (b + 255) & ~(size_t)255; return o; };
-    const size_t o_seed = take(4 * (size_t)qnum), o_fail = take(4 * (size_t)qnum), o_n = take(16);
-    const size_t o_q = take(4 * (size_t)qnum), o_kth = take(4 * (size_t)qnum);
-    const size_t o_ids = take(4 * (size_t)qnum * k), o_dis = take(4 * (size_t)qnum * k);
+    const size_t budget = search_budget(idx);
+    int qc = std::max(qnum, 1);
+    while (qc > 1 && plan_learned(qc, k).end > budget) qc = (qc + 1) / 2;
+    if (plan_learned(qc, k).end > budget) {
+        gts_set_error("scratch budget of %zu bytes is below the %zu bytes of one seeded query", budget,
+                      plan_learned(qc, k).end);
+        return GTS_ERR_NOMEM;
+    }
+    idx->last_fast_overflow = 0;
+    for (int q0 = 0; q0 < qnum; q0 += qc) {
+        const int n = std::min(qc, qnum - q0);
+        int rc = search_knn_plain_learned_chunk(idx, d_qids + q0, n, k, d_kth + q0,
+                                                d_ids ? d_ids + (size_t)q0 * k : nullptr,
+                                                d_dists ? d_dists + (size_t)q0 * k : nullptr, st);
+        if (rc) return rc;
+    }
+    return GTS_OK;
+}
+
+static int search_knn_plain_learned_chunk(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth,
+                                          int *d_ids, float *d_dists, cudaStream_t st)
+{
+    const LearnedPlan lp = plan_learned(qnum, k);
+    const size_t o_seed = lp.seed, o_fail = lp.fail, o_n = lp.n, o_q = lp.q, o_kth = lp.kth, o_ids = lp.ids,
+                 o_dis = lp.dis, off = lp.end;
     int rc;
     if ((rc = ensure_scratch(idx, off))) return rc;
     unsigned char *S = (unsigned char *)idx->scratch;
@@ -841,7 +886,7 @@ int search_knn_plain_learned(gts_index *idx, const int *d_qids, int qnum, int k,
     int nf = 0;
     GTS_CUDA_TRY(cudaMemcpyAsync(&nf, n_fail, sizeof(int), cudaMemcpyDeviceToHost, st));
     GTS_CUDA_TRY(cudaStreamSynchronize(st));
-    idx->last_fast_overflow = nf;
+    idx->last_fast_overflow += nf;
     if (nf == 0) return GTS_OK;
     k_gather_q<<<(nf + 255) / 256, 256, 0, st>>>(d_qids, fail, nf, sub_q);
     idx->kernel_launches++;

@@ -284,21 +284,34 @@ int update_run(gts_index *idx, const int *flags, const int *ids, int nops, float
             std::vector<int> fill(off.begin(), off.end() - 1);
             for (size_t e = 0; e < ne; e++) ents[(size_t)fill[P.src[e]]++] = P.life[e];
         }
+        // the entries stay resident; the queries run in batches of 16 bytes
+        // each (id, time, two counts) within the call's budget
+        const size_t fixed = sizeof(int) * off.size() + sizeof(int4) * ne + 1024;
+        const size_t budget = search_budget(idx);
+        if (fixed + 16 > budget) {
+            gts_set_error("scratch budget of %zu bytes is below the %zu bytes of the stream's entries", budget,
+                          fixed + 16);
+            return GTS_ERR_NOMEM;
+        }
+        const int qc = (int)std::min<size_t>((size_t)nq, (budget - fixed) / 16);
         DevScratch sc;
         int *d_off = nullptr, *d_q = nullptr, *d_t = nullptr, *d_ct = nullptr, *d_cc = nullptr;
         int4 *d_ents = nullptr;
         if ((rc = sc.alloc(&d_off, off.size())) || (rc = sc.alloc(&d_ents, ne)) ||
-            (rc = sc.alloc(&d_q, (size_t)nq)) || (rc = sc.alloc(&d_t, (size_t)nq)) ||
-            (rc = sc.alloc(&d_ct, (size_t)nq)) || (rc = sc.alloc(&d_cc, (size_t)nq)))
+            (rc = sc.alloc(&d_q, (size_t)qc)) || (rc = sc.alloc(&d_t, (size_t)qc)) ||
+            (rc = sc.alloc(&d_ct, (size_t)qc)) || (rc = sc.alloc(&d_cc, (size_t)qc)))
             return rc;
         GTS_CUDA_TRY(cudaMemcpyAsync(d_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, s));
         GTS_CUDA_TRY(cudaMemcpyAsync(d_ents, ents.data(), sizeof(int4) * ne, cudaMemcpyHostToDevice, s));
-        GTS_CUDA_TRY(cudaMemcpyAsync(d_q, P.q_obj.data(), sizeof(int) * nq, cudaMemcpyHostToDevice, s));
-        GTS_CUDA_TRY(cudaMemcpyAsync(d_t, P.q_time.data(), sizeof(int) * nq, cudaMemcpyHostToDevice, s));
-        if ((rc = search_range_timed(idx, d_q, d_t, nq, r, d_off, d_ents, d_ct, d_cc, s))) return rc;
         std::vector<int> ct((size_t)nq), cc((size_t)nq);
-        GTS_CUDA_TRY(cudaMemcpyAsync(ct.data(), d_ct, sizeof(int) * nq, cudaMemcpyDeviceToHost, s));
-        GTS_CUDA_TRY(cudaMemcpyAsync(cc.data(), d_cc, sizeof(int) * nq, cudaMemcpyDeviceToHost, s));
+        for (int q0 = 0; q0 < nq; q0 += qc) {
+            const int n = std::min(qc, nq - q0);
+            GTS_CUDA_TRY(cudaMemcpyAsync(d_q, P.q_obj.data() + q0, sizeof(int) * n, cudaMemcpyHostToDevice, s));
+            GTS_CUDA_TRY(cudaMemcpyAsync(d_t, P.q_time.data() + q0, sizeof(int) * n, cudaMemcpyHostToDevice, s));
+            if ((rc = search_range_timed(idx, d_q, d_t, n, r, d_off, d_ents, d_ct, d_cc, s))) return rc;
+            GTS_CUDA_TRY(cudaMemcpyAsync(ct.data() + q0, d_ct, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+            GTS_CUDA_TRY(cudaMemcpyAsync(cc.data() + q0, d_cc, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+        }
         GTS_CUDA_TRY(cudaStreamSynchronize(s));
         int rnum = 0;   // the cache count of the last query that had a cache (update.cuh:592-597)
         for (int j = 0; j < nq; j++) {

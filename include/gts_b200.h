@@ -54,7 +54,12 @@ typedef struct {
     int dis_code;        /* DIS_CODE,   default 100 */
     int infi_dis;        /* INFI_DIS,   default 10000 */
     int max_in_size;     /* MAX_IN_SIZE (cache list), default 10 */
-    double mem_budget_gb;/* scratch budget per search call; 0 = 8 GB */
+    double mem_budget_gb;/* device scratch one search call may hold, in GiB (0 = 8): the fast
+                            form runs its queries in runs whose scratch fits (at most 32,768
+                            queries, halved in 128-query tiles), the seeded plain form in
+                            chunks, the update path its queries in batches; a call that cannot
+                            fit one tile / query returns GTS_ERR_NOMEM.  The plain traversal
+                            itself holds no per-query device memory.  Negative: invalid. */
 } gts_params;
 
 typedef struct {
@@ -200,10 +205,14 @@ int gts_knn_device(gts_index *idx, const int *d_qids, int qnum, int k, int form,
  * scratch is a fixed 12 MiB file-scope device array per device, so at most
  * 512 queries per call (more -> GTS_ERR_INVALID), L2 only, dim <= 128,
  * 1 <= k <= 64.  The index must already hold its filter records (made by
- * one earlier GTS_FORM_FAST gts_knn / gts_knn_device call).  The first call
- * on a device looks the array up (cudaGetSymbolAddress) and should come
- * before any stream capture.  All calls on a device share the array: calls
- * that overlap on the GPU race. */
+ * gts_index_prepare or one earlier GTS_FORM_FAST gts_knn / gts_knn_device
+ * call); a rebuild or gts_update_run drops them, so one of those must follow
+ * every update.  The array also holds the run's per-tile block lists, so
+ * past about 35 million objects 512 queries no longer fit ("fixed scratch
+ * ... too small"; fewer queries per call do).  Every call looks the array's
+ * address up (cudaGetSymbolAddress); the first call on a device loads the
+ * module and should come before any stream capture.  All calls on a device
+ * share the array: calls that overlap on the GPU race. */
 int gts_knn_device_noalloc(gts_index *idx, const int *d_qids, int qnum, int k,
                            float *d_kth, int *d_ids, float *d_dists, void *stream);
 

@@ -112,3 +112,12 @@ def test_argument_checks_need_no_device():
     assert lib.gts_fast_config_set(None, 8, 0, 4, 16) == -1
     msg = lib.gts_last_error()
     assert msg
+
+
+def test_negative_scratch_budget_is_rejected_before_the_device():
+    """gts_params.mem_budget_gb < 0 is an argument error (checked before any
+    device work, so it fails the same way with or without a GPU)."""
+    rows = G.gmm_rows(50, 4, 2, 0.5, 1)
+    with pytest.raises(gts.GtsError) as e:
+        gts.Index(rows, 2, mem_budget_gb=-1.0)
+    assert e.value.code == -1 and "mem_budget_gb" in str(e.value)

@@ -14,6 +14,10 @@ CASES = [  # (n, dim, comps, sigma, nq, max_h)
     (7777, 100, 8, 0.25, 130, 4),      # dimension padded to 128 inside the filter
     (4000, 32, 4, 1.0, 129, 4),
     (3000, 128, 1, 0.05, 64, 4),       # one tight cluster: many near-ties
+    # above a padded dimension of 128 the filter streams K in 64-wide chunks
+    (6000, 300, 16, 0.3, 200, 4),      # the d = 300 configurations' width (kp 320, the limit)
+    (5000, 200, 8, 0.3, 130, 4),       # kp 256
+    (4000, 129, 8, 0.3, 64, 4),        # one past the resident form (kp 192)
 ]
 
 
@@ -44,8 +48,8 @@ def test_fast_equals_plain_and_counts_work():
 
 
 def test_fast_falls_back_outside_its_shape(oracle):
-    """Dimensions above the filter's limit and k above 64 take the plain path."""
-    rows = G.gmm_rows(3000, 200, 8, 0.3, seed=7)
+    """Dimensions above the filter's limit (320) and k above 64 take the plain path."""
+    rows = G.gmm_rows(3000, 400, 8, 0.3, seed=7)
     ds = oracle.Dataset(2, rows)
     q = G.query_ids(3000, 40, seed=8)
     with gts.Index(rows, 2, max_h=4) as idx:
@@ -128,7 +132,8 @@ def test_fast_exact_ties_from_duplicate_rows(oracle):
             np.testing.assert_array_equal(dis, bd, err_msg=f"k={k}")
 
 
-@pytest.mark.parametrize("n,dim,comps,sigma,max_h", [(20000, 128, 32, 0.2, 5), (7777, 100, 8, 0.25, 4)])
+@pytest.mark.parametrize("n,dim,comps,sigma,max_h", [(20000, 128, 32, 0.2, 5), (7777, 100, 8, 0.25, 4),
+                                                     (6000, 300, 16, 0.3, 4)])
 def test_fast_range_counts_equal_brute_force(oracle, n, dim, comps, sigma, max_h):
     """Range counts through the tensor-core filter equal exact brute force in
     the reference's range arithmetic and the plain traversal's counts, from
