@@ -332,6 +332,41 @@ class Index:
                                         C.c_void_p(d_kth), C.c_void_p(d_ids or None),
                                         C.c_void_p(d_dists or None), C.c_void_p(stream)))
 
+    def _query_data(self, queries):
+        if self.metric == 6:
+            strs, lens = queries
+            strs = np.ascontiguousarray(strs, dtype=np.uint8)
+            lens = np.ascontiguousarray(lens, dtype=np.int32)
+            if strs.ndim != 2 or strs.shape[1] != STR_STRIDE:
+                raise ValueError(f"query strings must be (n, {STR_STRIDE}) bytes")
+            return None, strs, lens, len(lens)
+        rows = np.ascontiguousarray(queries, dtype=np.float32)
+        if rows.ndim != 2:
+            raise ValueError("query rows must be (n, dim)")
+        return rows, None, None, rows.shape[0]
+
+    def knn_rows(self, queries, k: int, return_ids: bool = False):
+        """kNN of queries given as data (rows, or (strs, lens) for metric 6),
+        not object ids: no self match."""
+        rows, strs, lens, n = self._query_data(queries)
+        kth = np.empty(n, np.float32)
+        ids = np.empty((n, k), np.int32) if return_ids else None
+        dis = np.empty((n, k), np.float32) if return_ids else None
+        _check(self._lib.gts_knn_rows(self._h, _fp(rows) if rows is not None else None,
+                                      strs.ctypes.data_as(C.c_char_p) if strs is not None else None,
+                                      _ip(lens) if lens is not None else None, n, k, _fp(kth),
+                                      _ip(ids) if return_ids else None, _fp(dis) if return_ids else None))
+        return (kth, ids, dis) if return_ids else kth
+
+    def range_rows(self, queries, r: float) -> np.ndarray:
+        """Range counts of queries given as data (see knn_rows)."""
+        rows, strs, lens, n = self._query_data(queries)
+        out = np.empty(n, np.int32)
+        _check(self._lib.gts_range_rows(self._h, _fp(rows) if rows is not None else None,
+                                        strs.ctypes.data_as(C.c_char_p) if strs is not None else None,
+                                        _ip(lens) if lens is not None else None, n, C.c_float(r), _ip(out)))
+        return out
+
     def range(self, qids, r: float, form: int = FORM_PLAIN) -> np.ndarray:
         """Count of objects within r of each query (itself included);
         form=FORM_FAST runs the tensor-core filter (L2, dim <= 128)."""

@@ -667,3 +667,114 @@ extern "C" int gts_range_ids(gts_index *idx, const int *qids, int qnum, float r,
     }
     return GTS_OK;
 }
+
+// ---------------------------------------------------------------- queries given as data
+
+static int check_rows_args(const gts_index *idx, const void *qrows, const char *qstrs, const int *qlens, int qnum,
+                           const char *fn)
+{
+    if (!idx || qnum < 0) {
+        gts_set_error("%s: invalid argument", fn);
+        return GTS_ERR_INVALID;
+    }
+    if (qnum > 0 && (idx->metric == 6 ? (!qstrs || !qlens) : !qrows)) {
+        gts_set_error("%s: the index's metric takes query %s", fn, idx->metric == 6 ? "strings and lengths" : "rows");
+        return GTS_ERR_INVALID;
+    }
+    return GTS_OK;
+}
+
+extern "C" int gts_knn_rows_device(gts_index *idx, const float *d_qrows, const char *d_qstrs, const int *d_qlens,
+                                   int qnum, int k, float *d_kth, int *d_ids, float *d_dists, void *stream)
+{
+    int rc = check_rows_args(idx, d_qrows, d_qstrs, d_qlens, qnum, "gts_knn_rows_device");
+    if (rc) return rc;
+    if (qnum > 0 && !d_kth) {
+        gts_set_error("gts_knn_rows_device: kth output is null");
+        return GTS_ERR_INVALID;
+    }
+    if (qnum == 0) return GTS_OK;
+    return gts::search_knn_rows(idx, idx->metric == 6 ? nullptr : d_qrows, idx->metric == 6 ? d_qstrs : nullptr,
+                                idx->metric == 6 ? d_qlens : nullptr, qnum, k, d_kth, d_ids, d_dists,
+                                (cudaStream_t)stream);
+}
+
+// Host query data copied into idx->io: rows, or strings and their lengths.
+static int stage_query_data(gts_index *idx, const float *qrows, const char *qstrs, const int *qlens, int qnum,
+                            size_t out_bytes, size_t out2_bytes, void **bufs)
+{
+    const bool str = idx->metric == 6;
+    if (str) {
+        for (int i = 0; i < qnum; i++)
+            if (qlens[i] < 0 || qlens[i] > GTS_STR_STRIDE - 1) {
+                gts_set_error("query string %d has length %d (allowed 0..%d)", i, qlens[i], GTS_STR_STRIDE - 1);
+                return GTS_ERR_INVALID;
+            }
+    }
+    IoCarve io;
+    io.add(str ? (size_t)qnum * GTS_STR_STRIDE : sizeof(float) * (size_t)qnum * idx->dim);
+    io.add(str ? sizeof(int) * (size_t)qnum : 0);
+    io.add(out_bytes);
+    io.add(out2_bytes);
+    io.add(out2_bytes);
+    int rc = io.get(idx, bufs);
+    if (rc) return rc;
+    cudaStream_t s = idx->stream;
+    if (str) {
+        GTS_CUDA_TRY(cudaMemcpyAsync(bufs[0], qstrs, (size_t)qnum * GTS_STR_STRIDE, cudaMemcpyHostToDevice, s));
+        GTS_CUDA_TRY(cudaMemcpyAsync(bufs[1], qlens, sizeof(int) * (size_t)qnum, cudaMemcpyHostToDevice, s));
+    } else {
+        GTS_CUDA_TRY(cudaMemcpyAsync(bufs[0], qrows, sizeof(float) * (size_t)qnum * idx->dim, cudaMemcpyHostToDevice,
+                                     s));
+    }
+    return GTS_OK;
+}
+
+extern "C" int gts_knn_rows(gts_index *idx, const float *qrows, const char *qstrs, const int *qlens, int qnum, int k,
+                            float *kth_out, int *ids_out, float *dists_out)
+{
+    int rc = check_rows_args(idx, qrows, qstrs, qlens, qnum, "gts_knn_rows");
+    if (rc) return rc;
+    if (qnum > 0 && !kth_out) {
+        gts_set_error("gts_knn_rows: kth output is null");
+        return GTS_ERR_INVALID;
+    }
+    if (qnum == 0) return GTS_OK;
+    const size_t kk = (size_t)(k > 0 ? k : 1) * (size_t)qnum;
+    void *b[5];
+    if ((rc = stage_query_data(idx, qrows, qstrs, qlens, qnum, sizeof(float) * (size_t)qnum, sizeof(int) * kk, b)))
+        return rc;
+    const bool str = idx->metric == 6;
+    cudaStream_t s = idx->stream;
+    rc = gts::search_knn_rows(idx, str ? nullptr : (const float *)b[0], str ? (const char *)b[0] : nullptr,
+                              str ? (const int *)b[1] : nullptr, qnum, k, (float *)b[2],
+                              ids_out ? (int *)b[3] : nullptr, dists_out ? (float *)b[4] : nullptr, s);
+    if (rc) return rc;
+    GTS_CUDA_TRY(cudaMemcpyAsync(kth_out, b[2], sizeof(float) * (size_t)qnum, cudaMemcpyDeviceToHost, s));
+    if (ids_out) GTS_CUDA_TRY(cudaMemcpyAsync(ids_out, b[3], sizeof(int) * kk, cudaMemcpyDeviceToHost, s));
+    if (dists_out) GTS_CUDA_TRY(cudaMemcpyAsync(dists_out, b[4], sizeof(float) * kk, cudaMemcpyDeviceToHost, s));
+    GTS_CUDA_TRY(cudaStreamSynchronize(s));
+    return GTS_OK;
+}
+
+extern "C" int gts_range_rows(gts_index *idx, const float *qrows, const char *qstrs, const int *qlens, int qnum,
+                              float r, int *counts_out)
+{
+    int rc = check_rows_args(idx, qrows, qstrs, qlens, qnum, "gts_range_rows");
+    if (rc) return rc;
+    if (qnum > 0 && !counts_out) {
+        gts_set_error("gts_range_rows: counts output is null");
+        return GTS_ERR_INVALID;
+    }
+    if (qnum == 0) return GTS_OK;
+    void *b[5];
+    if ((rc = stage_query_data(idx, qrows, qstrs, qlens, qnum, sizeof(int) * (size_t)qnum, 0, b))) return rc;
+    const bool str = idx->metric == 6;
+    cudaStream_t s = idx->stream;
+    rc = gts::search_range_rows(idx, str ? nullptr : (const float *)b[0], str ? (const char *)b[0] : nullptr,
+                                str ? (const int *)b[1] : nullptr, qnum, r, (int *)b[2], s);
+    if (rc) return rc;
+    GTS_CUDA_TRY(cudaMemcpyAsync(counts_out, b[2], sizeof(int) * (size_t)qnum, cudaMemcpyDeviceToHost, s));
+    GTS_CUDA_TRY(cudaStreamSynchronize(s));
+    return GTS_OK;
+}

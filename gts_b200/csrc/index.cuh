@@ -107,6 +107,12 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
 int search_range_timed(gts_index *idx, const int *d_qids, const int *d_qtime, int qnum, float r,
                        const int *d_ent_off, const int4 *d_ents, int *d_tree_counts, int *d_cache_counts,
                        cudaStream_t s);
+// Queries given as data (rows, or strings with lengths), not ids: no self
+// match; the plain traversal.
+int search_knn_rows(gts_index *idx, const float *d_qrows, const char *d_qstrs, const int *d_qlens, int qnum, int k,
+                    float *d_kth, int *d_ids, float *d_dists, cudaStream_t s);
+int search_range_rows(gts_index *idx, const float *d_qrows, const char *d_qstrs, const int *d_qlens, int qnum,
+                      float r, int *d_counts, cudaStream_t s);
 int search_range_ids(gts_index *idx, const int *d_qids, int qnum, float r, int *d_counts,
                      int *d_ids, float *d_dists, const int *d_offsets, cudaStream_t s);
 

@@ -83,6 +83,12 @@ struct SearchArgs {
     const int *ent_off;
     const int4 *ents;
     int *counts2;
+    // queries given as data instead of ids (nullable): rows [qnum][dim], or
+    // strings [qnum][109] with lengths; such a query is no object of the
+    // index (no self match)
+    const float *qrows;
+    const char *qstrs;
+    const int *qlens;
     float rel_eps;   // relative pruning slack
     float abs_eps;   // absolute pruning slack
 };
@@ -106,6 +112,7 @@ struct __align__(16) SearchSmem {
     int cpos[kLeafObjCap];     // positions needing an exact value
     int nint, nleaf, ncpos;
     int top, ncand, q, qid, cnt, cnt2, tq, overflow;
+    const float *qsrc;         // the query row in global memory
     unsigned long long n_obj, n_piv, n_exact;
     double R;
 };
@@ -144,7 +151,7 @@ __device__ __forceinline__ double exact_obj(const SearchArgs &a, const SearchSme
         return (double)edit_dp(txt, n, s.qstr, s.qlen);
     }
     const float *row = t.trows + (size_t)pos * t.dim;
-    const float *q = t.dim <= kMaxDimSmem ? s.qrow : t.rows + (size_t)s.qid * t.dim;
+    const float *q = t.dim <= kMaxDimSmem ? s.qrow : s.qsrc;
     return acc == kAccF64 ? dist_row_f64(row, q, t.dim, t.metric)
                           : (double)dist_row_f32(row, q, t.dim, t.metric);
 }
@@ -160,7 +167,7 @@ __device__ __forceinline__ double exact_id(const SearchArgs &a, const SearchSmem
         return (double)edit_dp(txt, n, s.qstr, s.qlen);
     }
     const float *row = t.rows + (size_t)id * t.dim;
-    const float *q = t.dim <= kMaxDimSmem ? s.qrow : t.rows + (size_t)s.qid * t.dim;
+    const float *q = t.dim <= kMaxDimSmem ? s.qrow : s.qsrc;
     return acc == kAccF64 ? dist_row_f64(row, q, t.dim, t.metric)
                           : (double)dist_row_f32(row, q, t.dim, t.metric);
 }
@@ -352,8 +359,9 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
         __syncthreads();
         const int q = s.q;
         if (q >= a.qnum) break;
-        const int qid = a.qids[q];
-        if (qid < 0 || qid >= t.num) {   // device-API ids are checked here
+        const bool by_data = a.qrows || a.qstrs;
+        const int qid = by_data ? -1 : a.qids[q];
+        if (!by_data && (qid < 0 || qid >= t.num)) {   // device-API ids are checked here
             if (tid == 0) {
                 atomicMax(a.status, (int)kKsBadQuery);
                 if (a.mode == kModeKnn) a.kth[q] = __int_as_float(0x7fc00000);
@@ -380,8 +388,8 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
                        : (a.seed_r2_bits ? sqrt((double)__int_as_float(a.seed_r2_bits[q])) : DBL_MAX);
         }
         if (t.metric == kEdit) {
-            int m = min(max(t.lens[qid], 0), kStrStride - 1);
-            const char *src = t.strs + (size_t)qid * kStrStride;
+            int m = min(max(by_data ? a.qlens[q] : t.lens[qid], 0), kStrStride - 1);
+            const char *src = by_data ? a.qstrs + (size_t)q * kStrStride : t.strs + (size_t)qid * kStrStride;
             for (int i = tid; i < kStrStride; i += NT) s.qstr[i] = src[i];
             for (int c = tid; c < 256; c += NT) {
                 uint64_t bits = 0;
@@ -390,12 +398,14 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
                 s.peq[c] = bits;
             }
             if (tid == 0) s.qlen = m;
-        } else if (t.dim <= kMaxDimSmem) {
-            const float *src = t.rows + (size_t)qid * t.dim;
-            for (int i = tid; i < t.dim; i += NT) s.qrow[i] = src[i];
+        } else {
+            const float *src = by_data ? a.qrows + (size_t)q * t.dim : t.rows + (size_t)qid * t.dim;
+            if (tid == 0) s.qsrc = src;
+            if (t.dim <= kMaxDimSmem)
+                for (int i = tid; i < t.dim; i += NT) s.qrow[i] = src[i];
         }
         __syncthreads();
-        const float *qrow = t.dim <= kMaxDimSmem ? s.qrow : t.rows + (size_t)qid * t.dim;
+        const float *qrow = t.dim <= kMaxDimSmem ? s.qrow : s.qsrc;
 
         // ---- traversal
         for (;;) {
@@ -941,6 +951,40 @@ int search_range(gts_index *idx, const int *d_qids, int qnum, float r, int *d_co
     a.r = r;
     a.counts = d_counts;
     a.deleted = d_deleted;
+    return run_search(idx, a, st);
+}
+
+int search_knn_rows(gts_index *idx, const float *d_qrows, const char *d_qstrs, const int *d_qlens, int qnum, int k,
+                    float *d_kth, int *d_ids, float *d_dists, cudaStream_t st)
+{
+    if (k < 1 || k > kMaxK) {
+        gts_set_error("k must be in [1, %d], got %d", kMaxK, k);
+        return GTS_ERR_INVALID;
+    }
+    SearchArgs a{};
+    a.qnum = qnum;
+    a.mode = kModeKnn;
+    a.k = k;
+    a.kth = d_kth;
+    a.ids = d_ids;
+    a.dists = d_dists;
+    a.qrows = d_qrows;
+    a.qstrs = d_qstrs;
+    a.qlens = d_qlens;
+    return run_search(idx, a, st);
+}
+
+int search_range_rows(gts_index *idx, const float *d_qrows, const char *d_qstrs, const int *d_qlens, int qnum,
+                      float r, int *d_counts, cudaStream_t st)
+{
+    SearchArgs a{};
+    a.qnum = qnum;
+    a.mode = kModeRangeCount;
+    a.r = r;
+    a.counts = d_counts;
+    a.qrows = d_qrows;
+    a.qstrs = d_qstrs;
+    a.qlens = d_qlens;
     return run_search(idx, a, st);
 }
 

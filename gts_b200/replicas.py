@@ -62,15 +62,26 @@ def merge_topk(dists: np.ndarray, ids: np.ndarray, k: int, infi: float):
     return kth, out_i, out_d
 
 
-def sharded_knn(local_search, qids: np.ndarray, k: int, infi: float, dist, device=None):
+def shard_search(index, lo: int):
+    """The local search of a rank whose index holds objects [lo, lo + n) of
+    the global set: the shard's k nearest of query rows (not ids: a query
+    need not be in this shard), global ids, on the GPU (gts_knn_rows)."""
+    def search(qrows, k):
+        _, ids, dists = index.knn_rows(qrows, k, return_ids=True)
+        return np.where(ids >= 0, ids + lo, -1).astype(np.int32), dists
+    return search
+
+
+def sharded_knn(local_search, queries, k: int, infi: float, dist, device=None):
     """kNN over an object set split across the ranks of `dist`.
 
-    local_search(qids, k) -> (ids, dists): this rank's shard's k nearest per
-    query (global ids, ascending by (distance, id)).  One all-gather of the
-    (queries x k) distances and ids, then merge_topk.  Every rank returns the
-    global answer."""
+    local_search(queries, k) -> (ids, dists): this rank's shard's k nearest
+    per query (global ids, ascending by (distance, id)); queries are the
+    query rows every rank holds.  One all-gather of the (queries x k)
+    distances and ids, then merge_topk.  Every rank returns the global
+    answer."""
     import torch
-    ids, dists = local_search(qids, k)
+    ids, dists = local_search(queries, k)
     world = dist.get_world_size()
     td = torch.as_tensor(np.ascontiguousarray(dists, dtype=np.float32), device=device)
     ti = torch.as_tensor(np.ascontiguousarray(ids, dtype=np.int32), device=device)

@@ -216,6 +216,24 @@ int gts_knn_device(gts_index *idx, const int *d_qids, int qnum, int k, int form,
 int gts_knn_device_noalloc(gts_index *idx, const int *d_qids, int qnum, int k,
                            float *d_kth, int *d_ids, float *d_dists, void *stream);
 
+/* No counterpart in the reference (its queries are object ids,
+ * search_v2.cuh:975 qid_list).  kNN of queries given as data: qrows
+ * (qnum x dim floats) for metrics 0/1/2/5, or qstrs (qnum x GTS_STR_STRIDE
+ * bytes) and qlens (lengths <= 108) for metric 6.  A query is not an object
+ * of the index, so nothing matches it by id (an equal object is found at
+ * its distance 0).  Outputs as gts_knn; the plain traversal.  This is what a
+ * rank of an object-sharded index runs for queries it does not hold.  Host
+ * buffers; _device takes device buffers on `stream`. */
+int gts_knn_rows(gts_index *idx, const float *qrows, const char *qstrs, const int *qlens, int qnum, int k,
+                 float *kth_out, int *ids_out, float *dists_out);
+int gts_knn_rows_device(gts_index *idx, const float *d_qrows, const char *d_qstrs, const int *d_qlens, int qnum,
+                        int k, float *d_kth, int *d_ids, float *d_dists, void *stream);
+
+/* No counterpart in the reference.  Range counts of queries given as data
+ * (as gts_knn_rows): the number of objects within r of each query row. */
+int gts_range_rows(gts_index *idx, const float *qrows, const char *qstrs, const int *qlens, int qnum, float r,
+                   int *counts_out);
+
 /* searchIndexRnnV2 (search_v2.cuh:780-972) -> res.
  * counts_out[q]: number of objects within r of qids[q] (itself included). */
 int gts_range(gts_index *idx, const int *qids, int qnum, float r, int *counts_out);

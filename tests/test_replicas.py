@@ -4,7 +4,8 @@
   slowest rank's (all-reduce MAX);
 * object-sharded search: every rank's k nearest within its shard, one
   all-gather and a (distance, id) merge equal the exact answer over all
-  objects (the oracle's brute force stands in for each rank's GPU search).
+  objects (here the oracle's brute force stands in for each rank's GPU
+  search; tests/test_gpu_sharded.py runs the GPU one).
 """
 import os
 import socket
@@ -39,12 +40,13 @@ def _worker(rank, world, port, results):
         lo, hi = R.shard_bounds(len(rows), world, rank)
         qrows = rows[qids]
 
-        def local_search(q, k):
+        def local_search(qr, k):
             # the shard's k nearest for query rows that need not be in it:
             # append the query rows to the shard and search k + len(q) deep
             # (the appended rows take at most len(q) places), then keep the
             # shard's own objects
-            ds = O.Dataset(2, np.concatenate([rows[lo:hi], qrows]))
+            q = qr
+            ds = O.Dataset(2, np.concatenate([rows[lo:hi], qr]))
             qq = np.arange(hi - lo, hi - lo + len(q), dtype=np.int32)
             _, ids, dd = O.knn_brute(ds, qq, k + len(q))
             out_i = np.full((len(q), k), -1, np.int32)
@@ -57,7 +59,7 @@ def _worker(rank, world, port, results):
                     out_d[r, j] = d
             return out_i, out_d
 
-        kth, ids, dd = R.sharded_knn(local_search, qids, 5, 10000.0, dist)
+        kth, ids, dd = R.sharded_knn(local_search, qrows, 5, 10000.0, dist)
         results[rank] = (t, q_seed, kth, ids)
     finally:
         dist.destroy_process_group()
