@@ -576,7 +576,8 @@ def run_gts(args):
         for g in groups:
             if g["op"] == "knn":
                 c = idx.fast_config(int(g["p"]))
-                idx.set_fast_config(int(g["p"]), args.learned_seed == "on", c["col_groups"], c["item_blocks"])
+                idx.set_fast_config(int(g["p"]), args.learned_seed == "on", c["col_groups"], c["item_blocks"],
+                                    c["streamed"])
     clocks = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         flush_l2(torch, dev, flush)

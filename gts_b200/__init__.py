@@ -280,10 +280,10 @@ class Index:
 
     def fast_config(self, k: int) -> dict:
         """The autotuned (or default) fast-form configuration for k."""
-        v = [C.c_int() for _ in range(4)]
+        v = [C.c_int() for _ in range(5)]
         _check(self._lib.gts_fast_config(self._h, k, *[C.byref(x) for x in v]))
         return {"tuned": bool(v[0].value), "learned_seed": bool(v[1].value), "col_groups": v[2].value,
-                "item_blocks": v[3].value}
+                "item_blocks": v[3].value, "streamed": bool(v[4].value)}
 
     def fast_graphs(self, on=None) -> int:
         """Turn the captured filter graph on/off (None: leave it); returns the
@@ -292,9 +292,11 @@ class Index:
         _check(self._lib.gts_fast_graphs(self._h, -1 if on is None else int(bool(on)), C.byref(n)))
         return n.value
 
-    def set_fast_config(self, k: int, learned_seed: bool, col_groups: int, item_blocks: int = 16):
+    def set_fast_config(self, k: int, learned_seed: bool, col_groups: int, item_blocks: int = 16,
+                        streamed: bool = False):
         """Pin the fast-form configuration for k instead of tuning it."""
-        _check(self._lib.gts_fast_config_set(self._h, k, int(bool(learned_seed)), col_groups, item_blocks))
+        _check(self._lib.gts_fast_config_set(self._h, k, int(bool(learned_seed)), col_groups, item_blocks,
+                                             int(bool(streamed))))
 
     def fast_autotune_reset(self):
         _check(self._lib.gts_fast_autotune_reset(self._h))

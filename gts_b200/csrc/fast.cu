@@ -626,13 +626,14 @@ struct FastTileArgs {
     float r2lo;
     int *rcnt;
     int nsc;                     // streamed form: K-chunk stages
+    int stream;                  // streamed form also at kp <= kFResKp (autotuned)
 };
 
 constexpr int kFS = 3;         // block stages, each with its own TMEM accumulator
 constexpr int kFAccCols = 160; // TMEM columns between accumulators (kFN = 144 used)
 // Streamed form (kp > kFResKp): K-chunk stages (a.nsc of them, at most
 // kFSCMax) and, per accumulator, the block's record tail in its own buffer.
-constexpr int kFSCMax = 4;
+constexpr int kFSCMax = 6;
 constexpr uint32_t kFTailBytes = 1024u + 32u;   // w, dn, block scalars
 constexpr uint32_t kFTailPad = 1088u;
 
@@ -693,7 +694,7 @@ constexpr uint32_t kStagedUnused = 0xffffffffu;
 // thread, only the uncertain ones are listed; no bound heap.
 //
 // KS (kp > kFResKp, where a whole record does not fit a stage beside the
-// query tile): the producer streams each block's operand rows in 64-wide K
+// query tile; below it an autotuner choice): the producer streams each block's operand rows in 64-wide K
 // chunks through a.nsc chunk stages -- a stage is refilled as soon as the
 // MMAs reading it are done (tcgen05.commit on cfree), one unit behind the
 // MMA issue -- and copies the block's record tail (w, dn, scalars) into the
@@ -1465,38 +1466,45 @@ __global__ void k_scatter_results(const int *idx, int n, int k, const float *kth
 static int fast_cg(int k) { return k <= 32 ? 4 : 2; }
 
 // One configuration of the fast form: seed with the learned radius or not,
-// epilogue column groups (warps per query lane), blocks per work item.
+// epilogue column groups (warps per query lane), blocks per work item,
+// records streamed in K chunks (forced above kp = kFResKp) or resident.
 struct FastCfg {
     bool learned;
     int cg, item;
+    bool stream;
 };
 
-static int cfg_pack(const FastCfg &c) { return 1 | (c.learned ? 2 : 0) | (c.cg << 2) | (c.item << 8); }
-static FastCfg cfg_unpack(int v) { return FastCfg{(v & 2) != 0, (v >> 2) & 7, (v >> 8) & 63}; }
+static int cfg_pack(const FastCfg &c)
+{
+    return 1 | (c.learned ? 2 : 0) | (c.cg << 2) | (c.item << 8) | (c.stream ? 1 << 14 : 0);
+}
+static FastCfg cfg_unpack(int v) { return FastCfg{(v & 2) != 0, (v >> 2) & 7, (v >> 8) & 63, (v & (1 << 14)) != 0}; }
 
-static bool fast_tile_fits(const FastShape &fs, int cg, int k);
+static bool fast_tile_fits(const FastShape &fs, int cg, int k, bool stream);
 
 static FastCfg fast_default_cfg(const gts_index *idx, int k)
 {
     // measured on clustered data: the own-block seed is tight for small k,
     // the learned radius pays for its re-answers from k = 16 on; the column
     // groups are the most whose shared memory fits this dimension
+    const FastShape fs = fast_shape(idx->dim);
+    const bool stream = fs.kp > kFResKp;
     int cg = fast_cg(k);
-    while (cg > 1 && !fast_tile_fits(fast_shape(idx->dim), cg, k)) cg >>= 1;
-    return FastCfg{idx->mlp_ready && k >= 16, cg, 16};
+    while (cg > 1 && !fast_tile_fits(fs, cg, k, stream)) cg >>= 1;
+    return FastCfg{idx->mlp_ready && k >= 16, cg, 16, stream};
 }
 
 // Shared memory of the filter kernel before candidate staging: the query
 // tile, the block stages (whole records, or for kp > kFResKp nsc K-chunk
 // stages and three tail buffers), the bound heaps (k > 16) and the control
 // block.  nsc = 0 for the resident form.
-static size_t fast_tile_fixed_smem(const FastShape &fs, int cg, int k, bool heap_in_smem, int nsc)
+static size_t fast_tile_fixed_smem(const FastShape &fs, int cg, int k, bool heap_in_smem, int nsc, bool stream)
 {
     const uint32_t arec_pad = (fs.arec_bytes + 1023u) & ~1023u;
     const uint32_t rec_pad = (fs.rec_bytes + 1023u) & ~1023u;
     const size_t heap = heap_in_smem ? sizeof(unsigned short) * 128 * cg * (size_t)k : 0;
-    const size_t stages = fs.kp > kFResKp ? (size_t)nsc * kFChunkBytes + kFS * (size_t)kFTailPad
-                                          : kFS * (size_t)rec_pad;
+    const size_t stages = (fs.kp > kFResKp || stream) ? (size_t)nsc * kFChunkBytes + kFS * (size_t)kFTailPad
+                                                      : kFS * (size_t)rec_pad;
     return 1024 + (size_t)arec_pad + stages + heap + sizeof(FastCtl) + 64;
 }
 
@@ -1514,17 +1522,17 @@ static int fast_tile_stages(const FastShape &fs, int cg, int k, bool heap_in_sme
 {
     const size_t optin = (size_t)smem_optin();
     for (int nsc = kFSCMax; nsc >= 2; nsc--)
-        if (fast_tile_fixed_smem(fs, cg, k, heap_in_smem, nsc) + 4096 <= optin) return nsc;
+        if (fast_tile_fixed_smem(fs, cg, k, heap_in_smem, nsc, true) + 4096 <= optin) return nsc;
     return 0;
 }
 
 // The filter configuration (column groups cg, bound heap in shared memory
 // for k > 16) fits this index's shared-memory plan.
-static bool fast_tile_fits(const FastShape &fs, int cg, int k)
+static bool fast_tile_fits(const FastShape &fs, int cg, int k, bool stream)
 {
     const bool heap = k > 16;
-    if (fs.kp > kFResKp) return fast_tile_stages(fs, cg, k, heap) >= 2;
-    return fast_tile_fixed_smem(fs, cg, k, heap, 0) + 32 * sizeof(FastStaged) <= (size_t)smem_optin();
+    if (fs.kp > kFResKp || stream) return fast_tile_stages(fs, cg, k, heap) >= 2;
+    return fast_tile_fixed_smem(fs, cg, k, heap, 0, false) + 32 * sizeof(FastStaged) <= (size_t)smem_optin();
 }
 
 template <int CG, int KH, bool RANGE = false, bool KS = false>
@@ -1537,7 +1545,7 @@ static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
                       a.fs.kp, CG, a.k);
         return GTS_ERR_INVALID;
     }
-    const size_t fixed = fast_tile_fixed_smem(a.fs, CG, a.k, KH == 0, b.nsc);
+    const size_t fixed = fast_tile_fixed_smem(a.fs, CG, a.k, KH == 0, b.nsc, KS);
     const int optin = smem_optin();
     b.st_cap = (int)std::min<size_t>(kFStageMax, optin > (int)fixed ? ((size_t)optin - fixed) / sizeof(FastStaged) : 0);
     b.st_cap &= ~31;
@@ -1556,8 +1564,8 @@ static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
 template <int CG, int KH, bool RANGE = false>
 static int launch_fast_tile_ks(const FastTileArgs &a, int grid, cudaStream_t st)
 {
-    return a.fs.kp > kFResKp ? launch_fast_tile_cg<CG, KH, RANGE, true>(a, grid, st)
-                             : launch_fast_tile_cg<CG, KH, RANGE, false>(a, grid, st);
+    return (a.fs.kp > kFResKp || a.stream) ? launch_fast_tile_cg<CG, KH, RANGE, true>(a, grid, st)
+                                           : launch_fast_tile_cg<CG, KH, RANGE, false>(a, grid, st);
 }
 
 static int launch_fast_tile(const FastTileArgs &a, int cg, int grid, cudaStream_t st)
@@ -1758,6 +1766,7 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     a.nbcap = nb;
     a.k = k;
     a.item = cfg.item;
+    a.stream = cfg.stream ? 1 : 0;
     a.fs = fs;
     a.cand_pos = r.cpos;
     a.cand_lb = r.clb;
@@ -2043,9 +2052,10 @@ static int fast_autotune(gts_index *idx, FastCall &fc, int qc, const int *d_qids
     for (int learned = 0; learned <= (idx->mlp_ready ? 1 : 0) && rc == GTS_OK; learned++)
         for (int cg = 4; cg >= 1 && rc == GTS_OK; cg >>= 1) {
             if (k > 16 && cg * k > 128) continue;   // heaps: 128 cg threads x k x 2 bytes <= 32 KB
-            if (!fast_tile_fits(fast_shape(idx->dim), cg, k)) continue;
-            for (int item = 8; item <= kFItemMax && rc == GTS_OK; item *= 2) {
-                const FastCfg c{learned != 0, cg, item};
+            for (int item = 8; item <= kFItemMax && rc == GTS_OK; item *= 2)
+            for (int stream = fast_shape(idx->dim).kp > kFResKp ? 1 : 0; stream <= 1 && rc == GTS_OK; stream++) {
+                if (!fast_tile_fits(fast_shape(idx->dim), cg, k, stream != 0)) continue;
+                const FastCfg c{learned != 0, cg, item, stream != 0};
                 if ((rc = (int)cudaEventRecord(e0, st)) != 0) {
                     rc = GTS_ERR_CUDA;
                     break;
@@ -2341,6 +2351,7 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
         a.nbcap = nb;
         a.k = 1;
         a.item = 16;
+        a.stream = 0;
         a.fs = fs;
         a.cand_pos = rb.cpos;
         a.cand_lb = rb.clb;
@@ -2391,7 +2402,7 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
     return GTS_OK;
 }
 
-int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *cg, int *item)
+int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *cg, int *item, int *streamed)
 {
     if (k < 1 || k > kFMaxK) {
         gts_set_error("k must be in [1, %d], got %d", kFMaxK, k);
@@ -2403,21 +2414,23 @@ int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *
     if (learned) *learned = c.learned ? 1 : 0;
     if (cg) *cg = c.cg;
     if (item) *item = c.item;
+    if (streamed) *streamed = c.stream ? 1 : 0;
     return GTS_OK;
 }
 
 }  // namespace gts
 
-extern "C" int gts_fast_config(const gts_index *idx, int k, int *tuned, int *learned, int *col_groups, int *item_blocks)
+extern "C" int gts_fast_config(const gts_index *idx, int k, int *tuned, int *learned, int *col_groups, int *item_blocks,
+                               int *streamed)
 {
     if (!idx) {
         gts_set_error("null index");
         return GTS_ERR_INVALID;
     }
-    return gts::fast_config_get(idx, k, tuned, learned, col_groups, item_blocks);
+    return gts::fast_config_get(idx, k, tuned, learned, col_groups, item_blocks, streamed);
 }
 
-extern "C" int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int item_blocks)
+extern "C" int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int item_blocks, int streamed)
 {
     if (!idx || k < 1 || k > gts::kFMaxK || (col_groups != 1 && col_groups != 2 && col_groups != 4) ||
         col_groups * k > 128 || (item_blocks != 8 && item_blocks != 16 && item_blocks != 32)) {
@@ -2425,13 +2438,14 @@ extern "C" int gts_fast_config_set(gts_index *idx, int k, int learned, int col_g
                       "8/16/32 blocks per item");
         return GTS_ERR_INVALID;
     }
+    const bool stream = streamed != 0 || gts::fast_shape(idx->dim).kp > gts::kFResKp;
     if (idx->metric == gts::kL2 && idx->dim <= gts::kFMaxKp &&
-        !gts::fast_tile_fits(gts::fast_shape(idx->dim), col_groups, k)) {
+        !gts::fast_tile_fits(gts::fast_shape(idx->dim), col_groups, k, stream)) {
         gts_set_error("gts_fast_config_set: %d column groups at k %d do not fit the shared memory at dim %d",
                       col_groups, k, idx->dim);
         return GTS_ERR_INVALID;
     }
-    idx->fast_cfg[k] = gts::cfg_pack(gts::FastCfg{learned != 0, col_groups, item_blocks});
+    idx->fast_cfg[k] = gts::cfg_pack(gts::FastCfg{learned != 0, col_groups, item_blocks, stream});
     return GTS_OK;
 }
 

@@ -139,7 +139,7 @@ int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d
                     float *d_dists, cudaStream_t s);
 int search_knn_plain_learned(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                              float *d_dists, cudaStream_t s);
-int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *cg, int *item);
+int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *cg, int *item, int *streamed);
 int fast_prepare_now(gts_index *idx, cudaStream_t st, int *done);
 // Drop the captured filter graph (its device pointers or parameters changed).
 void graph_invalidate(gts_index *idx);

@@ -153,14 +153,19 @@ int gts_kernel_launches(const gts_index *idx, long long *count);
  * used for k on this index.  The first batch of at least 2048 queries with a
  * given k is run once per candidate -- learned-radius seed on or off (when a
  * model is trained), 4 / 2 / 1 epilogue warps per query lane, 8 / 16 / 32
- * blocks per work item -- and the fastest is kept (every candidate returns
- * the same exact answers).  *tuned = 0 reports the default that smaller
- * batches use.  Any output pointer may be NULL. */
-int gts_fast_config(const gts_index *idx, int k, int *tuned, int *learned, int *col_groups, int *item_blocks);
+ * blocks per work item, block records resident per stage or streamed in
+ * 64-wide K chunks (*streamed; always streamed above dim 128) -- and the
+ * fastest that fits the shared memory is kept (every candidate returns the
+ * same exact answers).  *tuned = 0 reports the default that smaller batches
+ * use.  Any output pointer may be NULL. */
+int gts_fast_config(const gts_index *idx, int k, int *tuned, int *learned, int *col_groups, int *item_blocks,
+                    int *streamed);
 
 /* Pin the configuration for k (learned seed 0/1, 1/2/4 column groups with
- * groups * k <= 128, 8/16/32 blocks per item) instead of tuning it. */
-int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int item_blocks);
+ * groups * k <= 128, 8/16/32 blocks per item, streamed 0/1) instead of
+ * tuning it; GTS_ERR_INVALID when it does not fit this index's shared
+ * memory plan. */
+int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int item_blocks, int streamed);
 
 /* Forget the tuned configurations (the next large batch tunes again). */
 int gts_fast_autotune_reset(gts_index *idx);

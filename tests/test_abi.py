@@ -109,7 +109,7 @@ def test_argument_checks_need_no_device():
     assert lib.gts_range_form(None, ip, 4, C.c_float(1.0), 1, op) == -1
     assert lib.gts_range_form_device(None, ip, 4, C.c_float(1.0), 0, op, None) == -1
     assert lib.gts_plain_threads_set(None, 0, 256) == -1
-    assert lib.gts_fast_config_set(None, 8, 0, 4, 16) == -1
+    assert lib.gts_fast_config_set(None, 8, 0, 4, 16, 0) == -1
     msg = lib.gts_last_error()
     assert msg
 

@@ -185,3 +185,21 @@ def test_fast_range_extremes_and_device_entry(oracle):
         torch.cuda.synchronize()
         np.testing.assert_array_equal(d_c.cpu().numpy(), host)
         np.testing.assert_array_equal(host, oracle.range_brute(ds, q, r))
+
+
+def test_streamed_records_at_resident_widths_equal_brute_force(oracle):
+    """The streamed filter (records in 64-wide K chunks through their own
+    stages) pinned at widths where the resident form also fits gives the
+    same exact answers, for every column-group count that fits."""
+    rows = G.gmm_rows(15000, 128, 24, 0.25, seed=101)
+    ds = oracle.Dataset(2, rows)
+    q = G.query_ids(15000, 400, seed=102)
+    with gts.Index(rows, 2, max_h=5) as idx:
+        for k, cg in ((1, 4), (8, 4), (8, 1), (16, 2), (33, 2), (64, 1)):
+            idx.set_fast_config(k, False, cg, 8, streamed=True)
+            assert idx.fast_config(k)["streamed"]
+            kth, ids, dis = idx.knn(q, k, form=gts.FORM_FAST, return_ids=True)
+            bk, bi, bd = oracle.knn_brute(ds, q, k)
+            np.testing.assert_array_equal(ids, bi, err_msg=f"k={k} cg={cg}")
+            np.testing.assert_array_equal(kth, bk, err_msg=f"k={k} cg={cg}")
+            np.testing.assert_array_equal(dis, bd, err_msg=f"k={k} cg={cg}")
