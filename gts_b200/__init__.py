@@ -312,6 +312,14 @@ class Index:
         """Pin the plain traversal's threads per query CTA (128/256/512, 0 = tune)."""
         _check(self._lib.gts_plain_threads_set(self._h, mode, threads))
 
+    def plain_split(self, objects: int | None = None) -> int:
+        """Set the range traversal's hand-over threshold (objects verified by
+        one query in one CTA; 0 = off; None leaves it); returns the number of
+        (query, node) items handed over so far."""
+        n = C.c_longlong()
+        _check(self._lib.gts_plain_split(self._h, -1 if objects is None else int(objects), C.byref(n)))
+        return n.value
+
     def kernel_launches(self) -> int:
         """Kernels this library launched for searches on this handle so far."""
         n = C.c_longlong()

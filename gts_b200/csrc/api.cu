@@ -379,6 +379,7 @@ extern "C" void gts_index_free(gts_index *idx)
     if (idx->d_status) cudaFree(idx->d_status);
     if (idx->d_stats) cudaFree(idx->d_stats);
     if (idx->scratch) cudaFree(idx->scratch);
+    if (idx->split_buf) cudaFree(idx->split_buf);
     if (idx->io) cudaFree(idx->io);
     if (idx->graph_exec) cudaGraphExecDestroy(idx->graph_exec);
     if (idx->graph_stream) cudaStreamDestroy(idx->graph_stream);
@@ -776,5 +777,16 @@ extern "C" int gts_range_rows(gts_index *idx, const float *qrows, const char *qs
     if (rc) return rc;
     GTS_CUDA_TRY(cudaMemcpyAsync(counts_out, b[2], sizeof(int) * (size_t)qnum, cudaMemcpyDeviceToHost, s));
     GTS_CUDA_TRY(cudaStreamSynchronize(s));
+    return GTS_OK;
+}
+
+extern "C" int gts_plain_split(gts_index *idx, int objects, long long *items_handed)
+{
+    if (!idx) {
+        gts_set_error("null index");
+        return GTS_ERR_INVALID;
+    }
+    if (objects >= 0) idx->plain_split = objects;
+    if (items_handed) *items_handed = idx->last_split_items;
     return GTS_OK;
 }

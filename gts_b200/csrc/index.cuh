@@ -44,6 +44,13 @@ struct gts_index {
     // autotuned threads per query CTA of the plain traversal per search mode
     // (kNN, range count, range ids; search.cu), 0 = not tuned
     int plain_nt[3] = {};
+    // range counts: objects a query verifies in one CTA before it hands its
+    // older stack entries over as (query, node) items (0: never); the item
+    // lists, and the items handed over since the last reset
+    int plain_split = 32768;
+    void *split_buf = nullptr;
+    size_t split_bytes = 0;
+    long long last_split_items = 0;
 
     // reusable per-call scratch (grown on demand, freed with the handle)
     void *scratch = nullptr;

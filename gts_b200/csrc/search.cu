@@ -89,6 +89,20 @@ struct SearchArgs {
     const float *qrows;
     const char *qstrs;
     const int *qlens;
+    // (query, node) work items, range counts only (count and timed modes):
+    // items_in (nullable) are (query, node, first unverified object, lower
+    // bound bits) handed over by an earlier launch; n_items_in of them are
+    // the work units instead of the queries.  A query that has verified more
+    // than split_objs objects in one CTA since its last hand-over gives all
+    // but its kBatch newest stack entries to items_out (capacity items_cap,
+    // count in *n_items_out; entries with query -1 are unused), so the next
+    // launch spreads its subtrees over every CTA.  With splitting on, counts
+    // are added atomically (the caller zeroes them first).
+    const int4 *items_in;
+    int4 *items_out;
+    int *n_items_out;
+    int items_cap;
+    int split_objs;   // 0: no hand-over
     float rel_eps;   // relative pruning slack
     float abs_eps;   // absolute pruning slack
 };
@@ -113,7 +127,7 @@ struct __align__(16) SearchSmem {
     int nint, nleaf, ncpos;
     int top, ncand, q, qid, cnt, cnt2, tq, overflow;
     const float *qsrc;         // the query row in global memory
-    unsigned long long n_obj, n_piv, n_exact;
+    unsigned long long n_obj, n_piv, n_exact, obj_mark;
     double R;
 };
 
@@ -357,8 +371,14 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
     for (;;) {
         if (tid == 0) s.q = atomicAdd(a.counter, 1);
         __syncthreads();
-        const int q = s.q;
-        if (q >= a.qnum) break;
+        const int w = s.q;   // work unit: a query, or a handed-over (query, node) item
+        if (w >= a.qnum) break;
+        const int4 item = a.items_in ? a.items_in[w] : make_int4(w, 0, 0, 0);
+        const int q = item.x;
+        if (q < 0) {   // an unused item slot
+            __syncthreads();
+            continue;
+        }
         const bool by_data = a.qrows || a.qstrs;
         const int qid = by_data ? -1 : a.qids[q];
         if (!by_data && (qid < 0 || qid >= t.num)) {   // device-API ids are checked here
@@ -375,15 +395,15 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
         if (tid == 0) {
             s.qid = qid;
             s.top = 1;
-            s.stack_node[0] = 0;
-            s.stack_off[0] = 0;
-            s.stack_lb[0] = 0.f;
+            s.stack_node[0] = item.y;
+            s.stack_off[0] = item.z;
+            s.stack_lb[0] = __int_as_float(item.w);
             s.ncand = 0;
             s.cnt = 0;
             s.cnt2 = 0;
             s.tq = timed ? a.qtime[q] : 0;
             s.overflow = 0;
-            s.n_obj = s.n_piv = s.n_exact = 0;
+            s.n_obj = s.n_piv = s.n_exact = s.obj_mark = 0;
             s.R = !knn ? (double)a.r
                        : (a.seed_r2_bits ? sqrt((double)__int_as_float(a.seed_r2_bits[q])) : DBL_MAX);
         }
@@ -409,6 +429,31 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
 
         // ---- traversal
         for (;;) {
+            if (warp == 0 && a.split_objs > 0 && s.top > kBatch && s.n_obj - s.obj_mark > (unsigned long long)a.split_objs) {
+                // hand the older stack entries over as (query, node) items
+                const int top = s.top, nd = top - kBatch;
+                int base = 0;
+                if (lane == 0) base = atomicAdd(a.n_items_out, nd);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base + nd <= a.items_cap) {
+                    for (int i = lane; i < nd; i += 32)
+                        a.items_out[base + i] = make_int4(q, s.stack_node[i], s.stack_off[i], __float_as_int(s.stack_lb[i]));
+                    // the kBatch newest entries move to the bottom (one per lane)
+                    const int kn = s.stack_node[nd + lane], ko = s.stack_off[nd + lane];
+                    const float kl = s.stack_lb[nd + lane];
+                    __syncwarp();
+                    s.stack_node[lane] = kn;
+                    s.stack_off[lane] = ko;
+                    s.stack_lb[lane] = kl;
+                    if (lane == 0) s.top = kBatch;
+                } else {
+                    // no room: keep them; mark this reservation's slots below the capacity unused
+                    for (int i = base + lane; i < a.items_cap && i < base + nd; i += 32)
+                        a.items_out[i] = make_int4(-1, 0, 0, 0);
+                }
+                if (lane == 0) s.obj_mark = s.n_obj;
+                __syncwarp();
+            }
             if (warp == 0) {
                 // pop, in parallel, the top kBatch (= 32) entries: lane i looks
                 // at entry top-1-i.  Entries whose bound no longer admits
@@ -625,8 +670,15 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
             }
             if (tid == 0 && k > 0) a.kth[q] = s.ncand >= k ? (float)s.cd[k - 1] : (float)t.infi_dis;
         } else if (tid == 0) {
-            if (count_only) a.counts[q] = s.cnt;
-            if (timed) a.counts2[q] = s.cnt2;
+            const bool add = a.split_objs > 0 || a.items_in;
+            if (count_only) {
+                if (add) atomicAdd(&a.counts[q], s.cnt);
+                else a.counts[q] = s.cnt;
+            }
+            if (timed) {
+                if (add) atomicAdd(&a.counts2[q], s.cnt2);
+                else a.counts2[q] = s.cnt2;
+            }
         }
         if (tid == 0) {
             if (s.overflow) atomicMax(a.status, (int)kKsStackOverflow);
@@ -634,7 +686,7 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
                 atomicAdd(&a.stats[0], s.n_obj);
                 atomicAdd(&a.stats[1], s.n_piv);
                 atomicAdd(&a.stats[2], s.n_exact);
-                atomicAdd(&a.stats[3], 1ull);
+                if (!a.items_in) atomicAdd(&a.stats[3], 1ull);
             }
         }
         __syncthreads();
@@ -699,6 +751,8 @@ static int plain_autotune(gts_index *idx, const SearchArgs &a, cudaStream_t st, 
     if (a.qnum < 2 * sample) return GTS_OK;
     SearchArgs t = a;
     t.seed_r2_bits = nullptr;
+    t.split_objs = 0;
+    t.items_in = nullptr;
     cudaEvent_t e0, e1;
     GTS_CUDA_TRY(cudaEventCreate(&e0));
     GTS_CUDA_TRY(cudaEventCreate(&e1));
@@ -750,6 +804,59 @@ extern "C" int gts_plain_threads_set(gts_index *idx, int mode, int threads)
     return GTS_OK;
 }
 
+// Range counts with (query, node) hand-over: the queries run, then the items
+// heavy queries handed over run as their own launch, spread over every CTA,
+// until none are handed over (at most kSplitPhases launches; the last one
+// hands nothing over).  Counts are added atomically from zero.  The two item
+// lists live in the handle's own buffer (not the search scratch, which a
+// caller such as the fast form's overflow path may hold).
+constexpr int kSplitPhases = 8;
+
+static int run_split_phases(gts_index *idx, const SearchArgs &a0, int nt, cudaStream_t st)
+{
+    const size_t budget = search_budget(idx);
+    const int cap = (int)std::max<size_t>(1024, std::min<size_t>((size_t)1 << 20, budget / 64));
+    const size_t list_bytes = ((sizeof(int4) * (size_t)cap) + 255) & ~(size_t)255;
+    const size_t need = 2 * list_bytes + 256;
+    if (idx->split_bytes < need) {
+        if (idx->split_buf) cudaFree(idx->split_buf);
+        idx->split_buf = nullptr;
+        idx->split_bytes = 0;
+        if (cudaMalloc(&idx->split_buf, need) != cudaSuccess) {
+            cudaGetLastError();
+            gts_set_error("cudaMalloc of %zu bytes for the work-item lists failed", need);
+            return GTS_ERR_NOMEM;
+        }
+        idx->split_bytes = need;
+    }
+    unsigned char *B = (unsigned char *)idx->split_buf;
+    int4 *lists[2] = {(int4 *)B, (int4 *)(B + list_bytes)};
+    int *nout = (int *)(B + 2 * list_bytes);
+    GTS_CUDA_TRY(cudaMemsetAsync(a0.counts, 0, sizeof(int) * (size_t)a0.qnum, st));
+    if (a0.counts2) GTS_CUDA_TRY(cudaMemsetAsync(a0.counts2, 0, sizeof(int) * (size_t)a0.qnum, st));
+    SearchArgs a = a0;
+    a.split_objs = idx->plain_split;
+    a.items_cap = cap;
+    int cur = 0, n = a0.qnum, rc;
+    for (int phase = 0; phase < kSplitPhases && n > 0; phase++) {
+        a.items_in = phase == 0 ? nullptr : lists[cur];
+        a.qnum = n;
+        a.items_out = lists[cur ^ 1];
+        a.n_items_out = nout + (cur ^ 1);
+        if (phase == kSplitPhases - 1) a.split_objs = 0;
+        GTS_CUDA_TRY(cudaMemsetAsync(a.n_items_out, 0, sizeof(int), st));
+        GTS_CUDA_TRY(cudaMemsetAsync(idx->d_counter, 0, sizeof(int), st));
+        if ((rc = launch_search(idx, a, nt, st))) return rc;
+        int handed = 0;
+        GTS_CUDA_TRY(cudaMemcpyAsync(&handed, a.n_items_out, sizeof(int), cudaMemcpyDeviceToHost, st));
+        GTS_CUDA_TRY(cudaStreamSynchronize(st));
+        n = std::min(handed, cap);
+        idx->last_split_items += n;
+        cur ^= 1;
+    }
+    return GTS_OK;
+}
+
 static int run_search(gts_index *idx, SearchArgs &a, cudaStream_t st)
 {
     if (a.qnum <= 0) return GTS_OK;
@@ -784,7 +891,8 @@ static int run_search(gts_index *idx, SearchArgs &a, cudaStream_t st)
         if (a.mode != kModeRangeIds) idx->plain_nt[slot] = nt;
     }
     if (!nt) nt = kPlainDefaultThreads;
-    int rc = launch_search(idx, a, nt, st);
+    const bool split = (a.mode == kModeRangeCount || a.mode == kModeRangeTimed) && idx->plain_split > 0;
+    int rc = split ? run_split_phases(idx, a, nt, st) : launch_search(idx, a, nt, st);
     if (rc) return rc;
     int status = 0;
     GTS_CUDA_TRY(cudaMemcpyAsync(&status, idx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));

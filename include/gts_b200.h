@@ -181,6 +181,16 @@ int gts_fast_autotune_reset(gts_index *idx);
 int gts_plain_threads(const gts_index *idx, int mode, int *threads);
 int gts_plain_threads_set(gts_index *idx, int mode, int threads);
 
+/* No counterpart in the reference (its list tables hold (query, node) pairs
+ * level by level, search_v2.cuh:40-151).  Range counts of the plain
+ * traversal run one query per CTA until a query has verified `objects`
+ * objects in its CTA; then its older pending subtrees are handed over as
+ * (query, node) work items, which the next launch spreads over every CTA
+ * (their counts add up), so a few heavy queries do not leave the GPU idle
+ * behind them.  objects = 0 turns this off, < 0 leaves it (default 32768).
+ * *items_handed (nullable): items handed over since the index was built. */
+int gts_plain_split(gts_index *idx, int objects, long long *items_handed);
+
 /* No counterpart in the reference (it launches and synchronises every kernel
  * from the host, search_v2.cuh:868-871).  A GTS_FORM_FAST batch of at most
  * 32,768 queries runs its filter pass as a CUDA graph, captured once per
@@ -272,12 +282,14 @@ int gts_range_ids(gts_index *idx, const int *qids, int qnum, float r, int *count
  * Train the kNN radius predictor of an L2 index: a 33-128-128-1 MLP whose
  * inputs are a query's distances to the first 32 pivots of the tree plus
  * log(k), and whose output is log of the k-th neighbour distance.  Labels are
- * exact radii of n_train random objects (k drawn from {1, 8, 32, 64} up to
- * k_max) computed by this index's own exact search; training runs on the
- * device (forward, backward and Adam kernels).  Afterwards GTS_FORM_FAST
- * searches start from the predicted radius, widened by the 99th percentile
- * of the held-out under-predictions, and re-answer any query whose radius
- * held fewer than k objects -- results stay exact.
+ * exact radii of n_train random objects (k drawn uniformly from
+ * {2, 4, 8, 16, 32, 64} up to k_max, plus k_max itself; k = 1 is not learned:
+ * its radius is 0, the query itself) computed by this index's own exact
+ * search; training runs on the device (forward, backward and Adam kernels).
+ * Afterwards GTS_FORM_FAST searches may start from the predicted radius
+ * (the autotuner decides per k; gts_fast_config), widened by the 99.5th
+ * percentile of the held-out under-predictions, and re-answer any query
+ * whose radius held fewer than k objects -- results stay exact.
  * val_rmse_log: RMS error of log(radius) on the held-out 10%; widen: factor
  * applied to predictions (both nullable).  A rebuild discards the model. */
 int gts_learn_radius(gts_index *idx, int n_train, int k_max, int epochs, unsigned seed,
