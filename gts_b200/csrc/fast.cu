@@ -589,16 +589,21 @@ __global__ void __launch_bounds__(256) k_need_blk(const float *__restrict__ qt,
 }
 
 // Work items: (tile, first list entry) per `item` needed blocks of a tile.
+// Longest first: the full items from the front of the array (count in
+// n_items[0]), each tile's partial last item from the back (count in
+// n_items[1]), so the persistent CTAs end on the short ones.
 __global__ void k_items(int ntiles, const int *__restrict__ bcnt, int nbcap, int item, int2 *__restrict__ items,
-                        int *__restrict__ n_items)
+                        int *__restrict__ n_items, int items_cap)
 {
     const int tile = blockIdx.x * blockDim.x + threadIdx.x;
     if (tile >= ntiles) return;
     const int cnt = min(bcnt[tile], nbcap);
-    const int nit = (cnt + item - 1) / item;
-    if (nit == 0) return;
-    const int base = atomicAdd(n_items, nit);
-    for (int i = 0; i < nit; i++) items[base + i] = make_int2(tile, i * item);
+    const int full = cnt / item, rem = cnt - full * item;
+    if (full > 0) {
+        const int base = atomicAdd(&n_items[0], full);
+        for (int i = 0; i < full; i++) items[base + i] = make_int2(tile, i * item);
+    }
+    if (rem > 0) items[items_cap - 1 - atomicAdd(&n_items[1], 1)] = make_int2(tile, full * item);
 }
 
 // ---------------------------------------------------------------- filter
@@ -608,8 +613,9 @@ struct FastTileArgs {
     const unsigned char *arec;   // query tile records
     const int *blist;            // [ntiles][nbcap] needed blocks per tile
     const int *bcnt;             // [ntiles]
-    const int2 *items;           // (tile, first entry)
-    const int *n_items;
+    const int2 *items;           // (tile, first entry): n_items[0] full ones from the front,
+    const int *n_items;          // n_items[1] partial ones from the back of items_cap
+    int items_cap;
     int nbcap, k;
     int item;                    // blocks per work item (<= kFItemMax)
     int st_cap;                  // staged candidates per item (shared memory)
@@ -766,8 +772,9 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
         if (t == 0) {
             const int it = atomicAdd(a.item_counter, 1);
             int tile = -1, nblk = 0;
-            if (it < *a.n_items) {
-                const int2 e = a.items[it];
+            const int nfull = a.n_items[0];
+            if (it < nfull + a.n_items[1]) {
+                const int2 e = it < nfull ? a.items[it] : a.items[a.items_cap - 1 - (it - nfull)];
                 tile = e.x;
                 nblk = min(a.item, min(a.bcnt[tile], a.nbcap) - e.y);
                 for (int j = 0; j < nblk; j++) ctl.blk[j] = a.blist[(size_t)tile * a.nbcap + e.y + j];
@@ -1649,12 +1656,19 @@ struct RunBufs {
     size_t cub_bytes;
 };
 
+// Work items of a run at most: every tile's needed blocks in items of the
+// smallest size.
+static size_t plan_items_cap(int ntiles, int nb)
+{
+    return std::max<size_t>((size_t)ntiles * ((nb + kFItemMin - 1) / kFItemMin), 1);
+}
+
 static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunBufs *b)
 {
     const FastShape fs = fast_shape(idx->dim);
     const int ntiles = (qnum + kFT - 1) / kFT;
     const int nb = idx->fast_nb, nsbw = (idx->fast_nsb + 31) / 32;
-    const size_t itemcap = (size_t)ntiles * ((nb + kFItemMin - 1) / kFItemMin);
+    const size_t itemcap = plan_items_cap(ntiles, nb);
     size_t cub_bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (int *)nullptr, (int *)nullptr, (int *)nullptr,
                                     (int *)nullptr, qnum, 0, 32, (cudaStream_t)0);
@@ -1670,7 +1684,7 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
     r.cub_ = (float *)take(4 * (size_t)qnum * kFCand);
     r.ccnt = (int *)take(4 * (size_t)qnum);
     r.r2 = (int *)take(4 * (size_t)qnum);
-    r.ctr = (int *)take(8 * sizeof(int));   // failures, item counter, item count
+    r.ctr = (int *)take(8 * sizeof(int));   // failures, item counter, full and partial item counts
     r.arec = take((size_t)ntiles * fs.arec_bytes);
     r.sb_mask = (uint32_t *)take(4 * (size_t)ntiles * std::max(nsbw, 1));
     r.qt = (float *)take(4 * (size_t)ntiles * fs.kp * kFT);
@@ -1752,7 +1766,8 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     k_need_blk<<<dim3(ntiles, need_y), 256, need_smem, st>>>(r.qt, r.arec, fs, bs, r.r2, r.sb_mask, nsbw,
                                                                r.blist, r.bcnt, nb, idx->d_stats);
     idx->kernel_launches++;
-    k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, r.bcnt, nb, cfg.item, r.items, r.ctr + 2);
+    k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, r.bcnt, nb, cfg.item, r.items, r.ctr + 2,
+                                                  (int)plan_items_cap(ntiles, nb));
     idx->kernel_launches++;
     GTS_CUDA_TRY(cudaGetLastError());
 
@@ -1763,6 +1778,7 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     a.bcnt = r.bcnt;
     a.items = r.items;
     a.n_items = r.ctr + 2;
+    a.items_cap = (int)plan_items_cap(ntiles, nb);
     a.nbcap = nb;
     a.k = k;
     a.item = cfg.item;
@@ -2339,7 +2355,8 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
         const int need_y = std::max(kNeedBlkY, std::min(32, (4 * nsm + ntiles - 1) / ntiles));
         k_need_blk<<<dim3(ntiles, need_y), 256, need_smem, st>>>(rb.qt, rb.arec, fs, bs, rb.r2, rb.sb_mask, nsbw,
                                                                  rb.blist, rb.bcnt, nb, idx->d_stats);
-        k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, rb.bcnt, nb, 16, rb.items, rb.ctr + 2);
+        k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, rb.bcnt, nb, 16, rb.items, rb.ctr + 2,
+                                                      (int)plan_items_cap(ntiles, nb));
         GTS_CUDA_TRY(cudaGetLastError());
         FastTileArgs a;
         a.recs = idx->fast_recs;
@@ -2348,6 +2365,7 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
         a.bcnt = rb.bcnt;
         a.items = rb.items;
         a.n_items = rb.ctr + 2;
+        a.items_cap = (int)plan_items_cap(ntiles, nb);
         a.nbcap = nb;
         a.k = 1;
         a.item = 16;
