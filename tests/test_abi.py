@@ -121,3 +121,49 @@ def test_negative_scratch_budget_is_rejected_before_the_device():
     with pytest.raises(gts.GtsError) as e:
         gts.Index(rows, 2, mem_budget_gb=-1.0)
     assert e.value.code == -1 and "mem_budget_gb" in str(e.value)
+
+
+def test_reference_compat_header_builds(tmp_path):
+    """include/gts_ref_compat.h (the reference's entry points over this
+    library) compiles as C++17 and links against libgts_b200 with the
+    reference's call shapes (no GPU needed to build)."""
+    src = tmp_path / "compat_main.cpp"
+    src.write_text(r'''
+#include "gts_ref/tree.cuh"
+#include "gts_ref/file.cuh"
+#include "gts_ref/search.cuh"
+#include "gts_ref/update.cuh"
+#include "gts_ref/search_v2.cuh"
+#include "gts_ref/config.cuh"
+int *data_info; short *data_d; char *data_s; int *size_s; int *qid_list; int qnum;
+int *max_node_num; int *id_list; TN *node_list; int tree_h; int *empty_list;
+int *qresult_count, *qresult_count_prefix, *result_id; float *result_dis;
+int main(int argc, char **argv) {
+    if (argc < 2) return 0;
+    load(argv[1], data_info, data_d, data_s, size_s);
+    loadQuery(argv[2], qid_list, qnum);
+    indexConstru(data_d, data_s, size_s, data_info, id_list, node_list, max_node_num, tree_h, empty_list);
+    searchIndexKnnV2(data_d, node_list, id_list, max_node_num, qid_list, qnum, 8, tree_h, data_info, empty_list, data_s, size_s);
+    searchIndexRnnV2(data_d, node_list, id_list, max_node_num, qid_list, qnum, 1.f, tree_h, data_info, empty_list, data_s, size_s);
+    float ts = 0; FILE *f = nullptr;
+    searchIndexRnn(data_d, node_list, id_list, max_node_num, qid_list, qnum, 1.f, tree_h, data_info, empty_list,
+                   qresult_count, qresult_count_prefix, result_id, result_dis, data_s, size_s, ts, f);
+    searchIndexKnn(data_d, node_list, id_list, max_node_num, qid_list, qnum, 4, tree_h, data_info, empty_list,
+                   result_id, result_dis, qresult_count, qresult_count_prefix, data_s, size_s, ts, f);
+    loadUpdate(argv[3], update_list, update_num);
+    float tu = 0; int cs = 0, cu = 0;
+    updateIndexRnn(data_d, node_list, id_list, max_node_num, qid_list, 1, 1.f, tree_h, data_info, empty_list,
+                   qresult_count, qresult_count_prefix, result_id, result_dis, data_s, size_s, f, ts, tu, cs, cu);
+    saveK(argv[4], argv[5], result_id, result_dis, 4, qnum);
+    return res[0] + (int)res_dis[0];
+}
+''')
+    inc = os.path.join(ROOT, "include")
+    libdir = os.path.dirname(gts.lib_path())
+    cuda_inc = "/usr/local/cuda/include"
+    cuda_lib = "/usr/local/cuda/lib64"
+    if not os.path.isdir(cuda_inc):
+        pytest.skip("CUDA headers not installed here")
+    p = subprocess.run(["g++", "-std=c++17", "-I", inc, "-I", cuda_inc, str(src), "-o", str(tmp_path / "compat"),
+                        "-L", libdir, "-lgts_b200", "-L", cuda_lib, "-lcudart"], capture_output=True, text=True)
+    assert p.returncode == 0, p.stderr[-3000:]
