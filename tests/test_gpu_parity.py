@@ -251,6 +251,23 @@ def test_gpu_equals_reference_goldens(oracle, name):
             np.testing.assert_array_equal(idx.range(qids, float(r)), fx[f"range_r{i}"])
 
 
+@pytest.mark.parametrize("name", [c for c in GI.cases() if c.startswith("l2_")])
+def test_fast_form_equals_reference_goldens(oracle, name):
+    """The tensor-core form pinned to the reference's own outputs (not only
+    through the oracle): k-th distances equal up to the reference's sort-code
+    quantum, range counts exactly."""
+    c, data, qids, radii, fx = GI.load_case(name)
+    with _index(c["metric"], data, max_h=c["max_h"]) as idx:
+        for k in c["ks"]:
+            got = idx.knn(qids, k, form=gts.FORM_FAST)
+            ref = fx[f"knn_k{k}"]
+            np.testing.assert_allclose(got, ref, rtol=0, atol=2e-6)
+            assert (got == ref).mean() > 0.98
+            np.testing.assert_array_equal(got, idx.knn(qids, k))   # = the plain form, exactly
+        for i, r in enumerate(radii):
+            np.testing.assert_array_equal(idx.range(qids, float(r), form=gts.FORM_FAST), fx[f"range_r{i}"])
+
+
 def test_gpu_on_reference_sample(oracle):
     d = GI.sample_dir()
     if d is None or not os.path.exists(os.path.join(GI.GOLDEN, "sample_knn_k8.txt")):

@@ -58,3 +58,25 @@ def test_noalloc_rejects_oversize_batch():
                                         C.c_void_p(out.data_ptr()), None, None, None)
         assert rc == -1  # GTS_ERR_INVALID
         assert b"exceed the maximum of 512" in lib.gts_last_error()
+
+
+def test_noalloc_equals_the_oracle_and_answers_overflowed_lists(oracle):
+    """Against exact brute force directly: 1,500 copies of one row make the
+    candidate list of every query among them overflow (every copy is at
+    distance 0), so the entry point's plain-traversal fallback answers
+    those; the other queries come from the filter.  Two calls in a row."""
+    torch = pytest.importorskip("torch")
+    lib = gts._load_lib()
+    base = G.gmm_rows(6000, 64, 8, 0.3, seed=36)
+    rows = np.concatenate([base, np.repeat(base[7:8], 1500, axis=0)])
+    ds = oracle.Dataset(2, rows)
+    q = np.concatenate([np.array([7, 6000, 6500, 7499], np.int32), G.query_ids(6000, 200, seed=37)])
+    with gts.Index(rows, 2, max_h=4) as idx:
+        idx.prepare(gts.FORM_FAST)
+        for k in (8, 20):
+            kth, ids, dis = _knn(lib, lib.gts_knn_device_noalloc, idx._h, q, k, torch)
+            assert idx.search_stats()["fallback"] >= 4     # the copies' lists overflowed
+            bk, bi, bd = oracle.knn_brute(ds, q, k)
+            np.testing.assert_array_equal(ids, bi, err_msg=f"k={k}")
+            np.testing.assert_array_equal(kth, bk, err_msg=f"k={k}")
+            np.testing.assert_array_equal(dis, bd, err_msg=f"k={k}")
