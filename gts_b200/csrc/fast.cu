@@ -1184,8 +1184,13 @@ constexpr int kFinB = 16;
 
 // KPM: the widest row the term buffer holds (kFResKp or kFMaxKp); FINB
 // candidates per batch (the buffer, FINB x (KPM + 1) doubles, stays within
-// the static shared memory).
-template <int KPM, int FINB>
+// the static shared memory).  CAP: the candidates one CTA holds.  Most
+// queries list fewer than 128, so a light variant (CAP = 128, a fraction of
+// the shared memory: twice the CTAs per SM to hide the row loads) runs
+// first over every query and lists the queries with more in `heavy`; the
+// full variant (CAP = kFCand) then runs over that list (`only`, *n_only of
+// them; CTAs past the count return at once).
+template <int KPM, int FINB, int CAP>
 __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ rows, int dim, int num,
                                                     const float *__restrict__ prow, int kp,
                                                     const int *__restrict__ ids_of_slot, int nslots,
@@ -1196,25 +1201,31 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
                                                     const int *__restrict__ cand_cnt,
                                                     const int *__restrict__ r2_bits, float *kth, int *ids,
                                                     float *dists, int *overflow, int *n_overflow,
-                                                    unsigned long long *stats)
+                                                    int *heavy, int *n_heavy, const int *only,
+                                                    const int *n_only, unsigned long long *stats)
 {
-    __shared__ double cd[kFCand];
-    __shared__ int cid[kFCand];
-    __shared__ int cl[kFCand];
+    __shared__ double cd[CAP];
+    __shared__ int cid[CAP];
+    __shared__ int cl[CAP];
     // the upper bounds (dead once the bound is set) share their space with the
     // pow terms; +1 double per row: lane c's reads of column j miss each
     // other's banks
     constexpr int kTermsBytes = FINB * (KPM + 1) * 8;
-    __shared__ __align__(16) unsigned char scratch[kTermsBytes > 4 * kFCand ? kTermsBytes : 4 * kFCand];
+    __shared__ __align__(16) unsigned char scratch[kTermsBytes > 4 * CAP ? kTermsBytes : 4 * CAP];
     float *ubs = reinterpret_cast<float *>(scratch);
     double(*terms)[KPM + 1] = reinterpret_cast<double(*)[KPM + 1]>(scratch);
     __shared__ int ns;
     __shared__ float kub;
-    const int q = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    if (only && (int)blockIdx.x >= *n_only) return;
+    const int q = only ? only[blockIdx.x] : (int)blockIdx.x;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int qid = qids[q];
     const int cnt = cand_cnt[q];
-    if (cnt > kFCand) {
-        if (t == 0) overflow[atomicAdd(n_overflow, 1)] = q;
+    if (cnt > CAP) {
+        if (t == 0) {
+            if (CAP < kFCand && cnt <= kFCand) heavy[atomicAdd(n_heavy, 1)] = q;
+            else overflow[atomicAdd(n_overflow, 1)] = q;
+        }
         return;
     }
     float R2 = __int_as_float(r2_bits[q]);
@@ -1646,7 +1657,7 @@ static int fast_prepare(gts_index *idx, cudaStream_t st)
 
 // Buffers of one filter run over qnum queries, carved from a region.
 struct RunBufs {
-    int *keys, *vals, *skeys, *order, *cpos, *ccnt, *r2, *ctr, *blist, *bcnt;
+    int *keys, *vals, *skeys, *order, *cpos, *ccnt, *r2, *ctr, *blist, *bcnt, *heavy;
     float *clb, *cub_;
     float *qt;   // [ntiles][kp][128] FP32 query rows of each tile
     unsigned char *arec;
@@ -1684,7 +1695,8 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
     r.cub_ = (float *)take(4 * (size_t)qnum * kFCand);
     r.ccnt = (int *)take(4 * (size_t)qnum);
     r.r2 = (int *)take(4 * (size_t)qnum);
-    r.ctr = (int *)take(8 * sizeof(int));   // failures, item counter, full and partial item counts
+    r.ctr = (int *)take(8 * sizeof(int));   // failures, item counter, full and partial item counts, heavy rechecks
+    r.heavy = (int *)take(4 * (size_t)qnum);
     r.arec = take((size_t)ntiles * fs.arec_bytes);
     r.sb_mask = (uint32_t *)take(4 * (size_t)ntiles * std::max(nsbw, 1));
     r.qt = (float *)take(4 * (size_t)ntiles * fs.kp * kFT);
@@ -1803,17 +1815,28 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
         GTS_CUDA_TRY(cudaEventRecordWithFlags(idx->fev[1], st, capturing ? cudaEventRecordExternal : 0));
     k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 1ull);
     idx->kernel_launches++;
-    if (fs.kp <= kFResKp)
-        k_fast_final<kFResKp, kFinB><<<qnum, 128, 0, st>>>(idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids,
-                                                          nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos, r.clb,
-                                                          r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr,
-                                                          idx->d_stats);
-    else
-        k_fast_final<kFMaxKp, kFinB / 2><<<qnum, 128, 0, st>>>(idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids,
-                                                              nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
-                                                              r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists,
-                                                              d_fail, r.ctr, idx->d_stats);
-    idx->kernel_launches++;
+    // light recheck over every query, then the full one over those with more
+    // than 128 candidates
+    if (fs.kp <= kFResKp) {
+        k_fast_final<kFResKp, kFinB, 128><<<qnum, 128, 0, st>>>(
+            idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
+            r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, r.heavy, r.ctr + 4, nullptr, nullptr,
+            idx->d_stats);
+        k_fast_final<kFResKp, kFinB, kFCand><<<qnum, 128, 0, st>>>(
+            idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
+            r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, nullptr, nullptr, r.heavy, r.ctr + 4,
+            idx->d_stats);
+    } else {
+        k_fast_final<kFMaxKp, kFinB / 2, 128><<<qnum, 128, 0, st>>>(
+            idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
+            r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, r.heavy, r.ctr + 4, nullptr, nullptr,
+            idx->d_stats);
+        k_fast_final<kFMaxKp, kFinB / 2, kFCand><<<qnum, 128, 0, st>>>(
+            idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
+            r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, nullptr, nullptr, r.heavy, r.ctr + 4,
+            idx->d_stats);
+    }
+    idx->kernel_launches += 2;
     GTS_CUDA_TRY(cudaGetLastError());
     return GTS_OK;
 }
@@ -1992,7 +2015,7 @@ static int fast_search_graph(gts_index *idx, FastCall &fc, const FastCfg &cfg, c
         }
         for (int i = 0; i < 8; i++) idx->graph_key[i] = key[i];
         // this library's kernels in the graph (CUB's and memsets not counted)
-        idx->graph_kernels = learned ? 12 : 11;
+        idx->graph_kernels = learned ? 13 : 12;
     } else {
         idx->graph_moved = false;
     }
