@@ -427,6 +427,19 @@ class Index:
         return {"params": P, "norm": norm, "ymu": float(extra[0]), "ysig": float(extra[1]),
                 "widen": float(extra[2])}
 
+    def update_run_rows(self, flags, ids, new_rows, r: float):
+        """The stream with inserts that bring new rows (flag 0 with id j
+        inserts new_rows[j]) -> (counts per query op, search s, update s)."""
+        f = np.ascontiguousarray(flags, dtype=np.int32)
+        i = np.ascontiguousarray(ids, dtype=np.int32)
+        nr = np.ascontiguousarray(new_rows, dtype=np.float32)
+        out = np.empty(max(1, int((f == 2).sum())), np.int32)
+        nq = C.c_int()
+        ts, tu = C.c_double(), C.c_double()
+        _check(self._lib.gts_update_run_rows(self._h, _ip(f), _ip(i), len(f), _fp(nr) if len(nr) else None, len(nr),
+                                             C.c_float(r), _ip(out), C.byref(nq), C.byref(ts), C.byref(tu)))
+        return out[:nq.value], ts.value, tu.value
+
     def update_run(self, flags, ids, r: float):
         """-> (counts per query op, search seconds, update seconds)."""
         f = np.ascontiguousarray(flags, dtype=np.int32)
@@ -439,23 +452,24 @@ class Index:
         return out[:nq.value], ts.value, tu.value
 
 
-def update_plan(num: int, flags, ids, max_in_size: int = 10) -> dict:
+def update_plan(num: int, flags, ids, max_in_size: int = 10, n_new: int = 0) -> dict:
     """The host pass of the stream update (updateIndexRnn's id bookkeeping,
     update.cuh:473-623) with no device work: per query op its data row, its
     operation index and whether the cache list held entries; per entry (the
     num data rows, then one copy per insert) the row it copies and its
     (tree_from, tree_to, cache_from, cache_to) operation intervals; the data
-    rows after the last compaction."""
+    rows after the last compaction.  n_new > 0: a flag-0 op with id j brings
+    new row j (object num + j) instead of copying a physical row."""
     f = np.ascontiguousarray(flags, dtype=np.int32)
     i = np.ascontiguousarray(ids, dtype=np.int32)
     nq_cap = max(1, int((f == 2).sum()))
-    ne_cap = num + int((f == 0).sum())
+    ne_cap = num + int((f == 0).sum()) + n_new
     q_obj, q_time, q_cache = (np.empty(nq_cap, np.int32) for _ in range(3))
     src = np.empty(ne_cap, np.int32)
     life = np.empty((ne_cap, 4), np.int32)
     final = np.empty(max(1, ne_cap), np.int32)
     nq, ne, nf = C.c_int(), C.c_int(), C.c_int()
-    _check(_load_lib().gts_update_plan(num, _ip(f), _ip(i), len(f), max_in_size, _ip(q_obj), _ip(q_time),
+    _check(_load_lib().gts_update_plan(num, _ip(f), _ip(i), len(f), max_in_size, n_new, _ip(q_obj), _ip(q_time),
                                        _ip(q_cache), C.byref(nq), _ip(src), _ip(life), C.byref(ne),
                                        _ip(final), C.byref(nf)))
     return {"q_obj": q_obj[:nq.value], "q_time": q_time[:nq.value], "q_cache": q_cache[:nq.value].astype(bool),

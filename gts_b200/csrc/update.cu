@@ -139,7 +139,11 @@ struct StreamPlan {
 // order.  fphys counts the entries live at the last compaction (their rank
 // is the physical id); flive the tree entries live now (their rank is the
 // logical id of a delete).
-int plan_stream(int n0, const int *flags, const int *ids, int nops, int max_in, StreamPlan *P)
+// new_base < 0: an insert copies physical row ids[i] (the reference);
+// otherwise it brings new row ids[i] (0 <= ids[i] < n_new), whose index
+// object is new_base + ids[i].
+int plan_stream(int n0, const int *flags, const int *ids, int nops, int max_in, int new_base, int n_new,
+                StreamPlan *P)
 {
     int n_ins = 0;
     for (int i = 0; i < nops; i++) n_ins += flags[i] == 0;
@@ -157,13 +161,14 @@ int plan_stream(int n0, const int *flags, const int *ids, int nops, int max_in, 
     std::vector<int> cache, pending;
     for (int i = 0; i < nops; i++) {
         const int f = flags[i];
-        if (f == 0) {   // insert: a copy of physical row ids[i] joins the cache list
-            if (ids[i] >= tree_size) {
-                gts_set_error("op %d inserts row %d, data has %d rows", i, ids[i], tree_size);
+        if (f == 0) {   // insert: a copy of physical row ids[i] (or new row ids[i]) joins the cache list
+            if (new_base < 0 ? ids[i] >= tree_size : (ids[i] < 0 || ids[i] >= n_new)) {
+                gts_set_error("op %d inserts %s %d (%d available)", i, new_base < 0 ? "row" : "new row", ids[i],
+                              new_base < 0 ? tree_size : n_new);
                 return GTS_ERR_INVALID;
             }
             const int e = (int)P->src.size();
-            P->src.push_back(P->src[fphys.select(ids[i])]);
+            P->src.push_back(new_base < 0 ? P->src[fphys.select(ids[i])] : new_base + ids[i]);
             P->life.push_back(make_int4(kNever, kNever, i, kNever));
             cache.push_back(e);
             if ((int)cache.size() == max_in) {   // compaction (update.cuh:484-540)
@@ -259,15 +264,41 @@ static int rebuild_on(gts_index *idx, const std::vector<int> &map, cudaStream_t 
     return build_tree(idx, s);
 }
 
+// new_rows (host, n_new x dim floats; nullable): inserts bring these rows.
+// They are known before the stream runs, so the index is first rebuilt on
+// the data rows followed by the new rows; a new row is an object of that
+// index whose only entries are its inserts (none: it never counts).
 int update_run(gts_index *idx, const int *flags, const int *ids, int nops, float r, int *counts_out,
-               int *nq_out, double *search_s, double *update_s)
+               int *nq_out, double *search_s, double *update_s, const float *new_rows, int n_new)
 {
     using clk = std::chrono::high_resolution_clock;
     cudaStream_t s = idx->stream;
     auto t0 = clk::now();
+    const int n_data = idx->num;
     StreamPlan P;
-    int rc = plan_stream(idx->num, flags, ids, nops, idx->params.max_in_size, &P);
+    int rc = plan_stream(n_data, flags, ids, nops, idx->params.max_in_size, new_rows ? n_data : -1, n_new, &P);
     if (rc) return rc;
+    if (new_rows && n_new > 0) {
+        // the data rows, then the new rows; the tree over both
+        float *all = nullptr;
+        size_t acct = 0;
+        const size_t dim = (size_t)idx->dim;
+        if ((rc = dev_alloc(&all, ((size_t)n_data + n_new) * dim, &acct))) return rc;
+        GTS_CUDA_TRY(cudaMemcpyAsync(all, idx->rows, sizeof(float) * n_data * dim, cudaMemcpyDeviceToDevice, s));
+        GTS_CUDA_TRY(cudaMemcpyAsync(all + (size_t)n_data * dim, new_rows, sizeof(float) * (size_t)n_new * dim,
+                                     cudaMemcpyHostToDevice, s));
+        GTS_CUDA_TRY(cudaStreamSynchronize(s));
+        cudaFree(idx->rows);
+        idx->rows = all;
+        free_tree(idx);
+        idx->num = n_data + n_new;
+        idx->device_bytes = acct;
+        if ((rc = build_tree(idx, s))) return rc;
+        if (P.final_rows.empty()) {   // no compaction: the handle keeps the data rows
+            P.final_rows.resize((size_t)n_data);
+            for (int i = 0; i < n_data; i++) P.final_rows[i] = i;
+        }
+    }
     const int nq = (int)P.q_obj.size();
     double t_update = std::chrono::duration<double>(clk::now() - t0).count();
     double t_search = 0;
@@ -333,11 +364,12 @@ int update_run(gts_index *idx, const int *flags, const int *ids, int nops, float
 
 }  // namespace gts
 
-extern "C" int gts_update_plan(int num, const int *flags, const int *ids, int nops, int max_in_size, int *q_obj,
-                               int *q_time, int *q_cache, int *n_q, int *ent_src, int *ent_life, int *n_ent,
-                               int *final_rows, int *n_final)
+extern "C" int gts_update_plan(int num, const int *flags, const int *ids, int nops, int max_in_size, int n_new,
+                               int *q_obj, int *q_time, int *q_cache, int *n_q, int *ent_src, int *ent_life,
+                               int *n_ent, int *final_rows, int *n_final)
 {
-    if (num < 1 || nops < 0 || max_in_size < 1 || (nops > 0 && (!flags || !ids)) || !n_q || !n_ent || !n_final) {
+    if (num < 1 || nops < 0 || max_in_size < 1 || n_new < 0 || (nops > 0 && (!flags || !ids)) || !n_q || !n_ent ||
+        !n_final) {
         gts_set_error("gts_update_plan: invalid argument");
         return GTS_ERR_INVALID;
     }
@@ -348,7 +380,7 @@ extern "C" int gts_update_plan(int num, const int *flags, const int *ids, int no
         }
     }
     gts::StreamPlan P;
-    int rc = gts::plan_stream(num, flags, ids, nops, max_in_size, &P);
+    int rc = gts::plan_stream(num, flags, ids, nops, max_in_size, n_new > 0 ? num : -1, n_new, &P);
     if (rc) return rc;
     *n_q = (int)P.q_obj.size();
     *n_ent = (int)P.src.size();
@@ -389,5 +421,30 @@ extern "C" int gts_update_run(gts_index *idx, const int *flags, const int *ids, 
             return GTS_ERR_INVALID;
         }
     }
-    return gts::update_run(idx, flags, ids, nops, r, counts_out, nq_out, search_s, update_s);
+    return gts::update_run(idx, flags, ids, nops, r, counts_out, nq_out, search_s, update_s, nullptr, 0);
+}
+
+extern "C" int gts_update_run_rows(gts_index *idx, const int *flags, const int *ids, int nops, const float *new_rows,
+                                   int n_new, float r, int *counts_out, int *nq_out, double *search_s,
+                                   double *update_s)
+{
+    if (!idx || nops < 0 || n_new < 0 || (nops > 0 && (!flags || !ids || !counts_out)) || (n_new > 0 && !new_rows)) {
+        gts_set_error("gts_update_run_rows: invalid argument");
+        return GTS_ERR_INVALID;
+    }
+    if (idx->metric == 6) {
+        gts_set_error("gts_update_run_rows: new rows need a row metric (not edit distance)");
+        return GTS_ERR_INVALID;
+    }
+    for (int i = 0; i < nops; i++) {
+        if (flags[i] < 0 || flags[i] > 2) {
+            gts_set_error("op %d has flag %d (expected 0, 1 or 2)", i, flags[i]);
+            return GTS_ERR_INVALID;
+        }
+        if (flags[i] == 0 && (ids[i] < 0 || ids[i] >= n_new)) {
+            gts_set_error("op %d inserts new row %d of %d", i, ids[i], n_new);
+            return GTS_ERR_INVALID;
+        }
+    }
+    return gts::update_run(idx, flags, ids, nops, r, counts_out, nq_out, search_s, update_s, new_rows, n_new);
 }

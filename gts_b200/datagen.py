@@ -166,6 +166,18 @@ def update_stream(n: int, n_ops: int, seed: int, max_in_size: int = 10,
     return flags, ids
 
 
+def update_stream_new_rows(n: int, n_ops: int, seed: int, max_in_size: int = 10, **kw):
+    """update_stream whose inserts bring new rows: (flags, ids) with every
+    flag-0 id replaced by the running insert number 0, 1, 2, ... (the row of
+    the new-row array it inserts); deletes and queries as update_stream's
+    (their validity does not depend on the inserted rows' contents)."""
+    flags, ids = update_stream(n, n_ops, seed, max_in_size, **kw)
+    ins = flags == 0
+    ids = ids.copy()
+    ids[ins] = np.arange(int(ins.sum()), dtype=np.int32)
+    return flags, ids
+
+
 class _Fenwick:
     """Counts of live rows; select(u) = physical index of the (u+1)-th live row."""
 

@@ -322,9 +322,11 @@ int gts_update_run(gts_index *idx, const int *flags, const int *ids, int nops, f
                    int *counts_out, int *nq_out, double *search_s, double *update_s);
 
 /* updateIndexRnn's bookkeeping (update.cuh:473-623) without the device:
- * the host pass of gts_update_run.  Every object the stream ever holds is
- * an entry: the num rows of the data (entries 0..num-1) and one copy per
- * insert, in insertion order.  ent_src[e] is the data row entry e copies;
+ * the host pass of gts_update_run (n_new = 0) and gts_update_run_rows
+ * (n_new > 0: a flag-0 op with id j brings new row j, object num + j).
+ * Every object the stream ever holds is an entry: the num rows of the data
+ * (entries 0..num-1) and one per insert, in insertion order.  ent_src[e] is
+ * the object entry e copies (a data row, or num + j for new row j);
  * ent_life[4e..4e+3] = (tree_from, tree_to, cache_from, cache_to): entry e
  * is in the tree at operation t when tree_from < t < tree_to and in the
  * cache list when cache_from < t < cache_to (INT_MAX = never).  Query op j
@@ -334,9 +336,20 @@ int gts_update_run(gts_index *idx, const int *flags, const int *ids, int nops, f
  * rows of the array after the last compaction (*n_final = 0: no
  * compaction).  Size q_* to the number of flag-2 ops and ent_* / final_rows
  * to num + the number of flag-0 ops; every output array may be NULL. */
-int gts_update_plan(int num, const int *flags, const int *ids, int nops, int max_in_size,
+int gts_update_plan(int num, const int *flags, const int *ids, int nops, int max_in_size, int n_new,
                     int *q_obj, int *q_time, int *q_cache, int *n_q,
                     int *ent_src, int *ent_life, int *n_ent, int *final_rows, int *n_final);
+
+/* updateIndexRnn's operations (update.cuh:449-638) with inserts that bring
+ * new rows instead of copying a physical row (the reference's insert can
+ * only copy, update.cuh:481, 186): a flag-0 op with id j inserts
+ * new_rows[j] (n_new rows of dim floats, host memory).  Deletes and queries
+ * keep the reference's id rules; the data after a compaction holds the live
+ * rows, then the cached new rows.  The handle is rebuilt on the data rows
+ * plus the new rows first, searched once for every query op, and ends on
+ * the data of the last compaction.  Row metrics only. */
+int gts_update_run_rows(gts_index *idx, const int *flags, const int *ids, int nops, const float *new_rows,
+                        int n_new, float r, int *counts_out, int *nq_out, double *search_s, double *update_s);
 
 #ifdef __cplusplus
 }

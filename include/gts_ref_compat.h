@@ -398,7 +398,7 @@ inline void updateIndexRnn(float *&data_d, TN *&node_list, int *&id_list, int *&
     // the data after the last compaction, from the stream's bookkeeping
     int n_ent = 0, n_final = 0, n_q = 0;
     std::vector<int> final_rows((size_t)num0 + n);
-    gts_ref::check(gts_update_plan(num0, flags.data(), ids.data(), n, MAX_IN_SIZE, nullptr, nullptr, nullptr,
+    gts_ref::check(gts_update_plan(num0, flags.data(), ids.data(), n, MAX_IN_SIZE, 0, nullptr, nullptr, nullptr,
                                    &n_q, nullptr, nullptr, &n_ent, final_rows.data(), &n_final),
                    "updateIndexRnn");
     std::vector<int> counts((size_t)(nq > 0 ? nq : 1));

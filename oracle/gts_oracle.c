@@ -752,3 +752,92 @@ int orc_update_run(const orc_data *d0, const orc_params *p, int max_in_size,
     free(rows); free(strs); free(lens);
     return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * Stream update whose inserts bring new rows (an extension: the reference's
+ * insert copies an existing physical row, update.cuh:481, 186).  Same op
+ * semantics as orc_update_run otherwise; exact counts (live rows scanned).
+ * The cache list holds copies of the inserted rows; the compaction appends
+ * them after the live rows, as getNewData does (update.cuh:159-217). */
+
+/* F32-site distance of two rows (search_naive.cuh:31-68), through orc_dist
+ * on a two-row scratch set: a first (the cached row), then b (the query). */
+static float row_pair_dist_f32(int dim, int metric, const float *a, const float *b, float *tmp)
+{
+    memcpy(tmp, a, sizeof(float) * (size_t)dim);
+    memcpy(tmp + dim, b, sizeof(float) * (size_t)dim);
+    orc_data two = {dim, 2, metric, tmp, NULL, NULL};
+    return (float)orc_dist(&two, 0, 1, ORC_ACC_F32);
+}
+
+int orc_update_run_rows(const orc_data *d0, int max_in_size, const int *flags, const int *ids, int nops,
+                        const float *new_rows, int n_new, float r, int *counts_out, int *nq_out)
+{
+    if (d0->metric == 6 || max_in_size < 1) return -1;
+    orc_data d = *d0;
+    const int dim = d.dim;
+    float *rows = (float *)malloc(sizeof(float) * (size_t)d.num * dim);
+    memcpy(rows, d0->rows, sizeof(float) * (size_t)d.num * dim);
+    d.rows = rows;
+    float *cache = (float *)malloc(sizeof(float) * (size_t)max_in_size * dim);
+    float *tmp = (float *)malloc(sizeof(float) * 2 * (size_t)dim);
+    int tree_size = d.num, in_size = 0, rnum = 0, delete_id = 0, nq = 0, rc = 0;
+    int *is_delete = (int *)calloc((size_t)tree_size, sizeof(int));
+    for (int i = 0; i < nops && rc == 0; i++) {
+        if (flags[i] == 0) {
+            if (ids[i] < 0 || ids[i] >= n_new) { rc = -2; break; }
+            memcpy(cache + (size_t)(in_size++) * dim, new_rows + (size_t)ids[i] * dim, sizeof(float) * (size_t)dim);
+            if (in_size == max_in_size) {
+                int live = 0;
+                for (int j = 0; j < tree_size; j++) live += !is_delete[j];
+                const int nn = live + in_size;
+                float *nr = (float *)malloc(sizeof(float) * (size_t)nn * dim);
+                int o = 0;
+                for (int j = 0; j < tree_size; j++)
+                    if (!is_delete[j]) memcpy(nr + (size_t)(o++) * dim, rows + (size_t)j * dim, sizeof(float) * (size_t)dim);
+                memcpy(nr + (size_t)o * dim, cache, sizeof(float) * (size_t)in_size * dim);
+                free(rows);
+                rows = nr;
+                d.rows = rows;
+                d.num = nn;
+                tree_size = nn;
+                free(is_delete);
+                is_delete = (int *)calloc((size_t)tree_size, sizeof(int));
+                in_size = 0;
+            }
+        } else if (flags[i] == 1) {
+            /* findIdx (update.cuh:118-143) */
+            int u = ids[i], del_before = 0, total_del = 0;
+            for (int j = 0; j < tree_size; j++) total_del += is_delete[j];
+            for (int j = 0; j < tree_size; j++) {
+                del_before += is_delete[j];
+                if (!is_delete[j] && j - del_before == u) delete_id = j;
+            }
+            for (int j = tree_size; j < tree_size + in_size; j++)
+                if (j - total_del == u) delete_id = j;
+            if (delete_id < tree_size) {
+                is_delete[delete_id] = 1;
+            } else if (in_size > 0) {
+                int e = delete_id - tree_size;
+                if (e >= in_size) e = in_size - 1;
+                memmove(cache + (size_t)e * dim, cache + (size_t)(e + 1) * dim,
+                        sizeof(float) * (size_t)(in_size - 1 - e) * dim);
+                in_size--;
+            }
+        } else {
+            const int qid = ids[i];
+            if (qid < 0 || qid >= tree_size) { rc = -3; break; }
+            const int c = live_range_count(&d, is_delete, qid, r);
+            if (in_size > 0) {
+                rnum = 0;
+                for (int j = 0; j < in_size; j++)
+                    if (row_pair_dist_f32(dim, d.metric, cache + (size_t)j * dim, rows + (size_t)qid * dim, tmp) <= r)
+                        rnum++;
+            }
+            counts_out[nq++] = c + rnum;
+        }
+    }
+    *nq_out = nq;
+    free(rows); free(cache); free(tmp); free(is_delete);
+    return rc;
+}

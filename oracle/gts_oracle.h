@@ -99,6 +99,12 @@ int orc_update_run(const orc_data *d, const orc_params *p, int max_in_size,
                    const int *flags, const int *ids, int nops, float r,
                    int exact, int *counts_out, int *nq_out);
 
+/* Stream update whose flag-0 ops insert new_rows[ids[i]] (n_new rows of
+ * dim floats) instead of a copy of a physical row: an extension, not a
+ * reference behaviour.  Exact counts; row metrics only (not 6). */
+int orc_update_run_rows(const orc_data *d, int max_in_size, const int *flags, const int *ids, int nops,
+                        const float *new_rows, int n_new, float r, int *counts_out, int *nq_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -152,6 +152,21 @@ def range_brute(ds, qids, r: float, nthreads: int = 0) -> np.ndarray:
     return out
 
 
+def update_run_rows(ds, max_in_size: int, flags, ids, new_rows, r: float) -> np.ndarray:
+    """Counts per query op of a stream whose inserts bring new rows
+    (flag 0 with id j inserts new_rows[j]); exact counts."""
+    f = np.ascontiguousarray(flags, dtype=np.int32)
+    i = np.ascontiguousarray(ids, dtype=np.int32)
+    nr = np.ascontiguousarray(new_rows, dtype=np.float32)
+    out = np.empty(int((f == 2).sum()) + 1, dtype=np.int32)
+    nq = C.c_int(0)
+    rc = lib().orc_update_run_rows(ds.ref, max_in_size, _iptr(f), _iptr(i), len(f), _fptr(nr), len(nr),
+                                   C.c_float(r), _iptr(out), C.byref(nq))
+    if rc != 0:
+        raise RuntimeError(f"orc_update_run_rows failed: {rc}")
+    return out[:nq.value]
+
+
 def update_run(ds, p, max_in_size: int, flags, ids, r: float, exact: bool = False) -> np.ndarray:
     """Counts per query op; exact=True scans live rows instead of the
     reference's v1 tree search (which skips oversized last-level nodes)."""

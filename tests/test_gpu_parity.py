@@ -177,6 +177,27 @@ def test_update_equals_oracle(oracle):
     np.testing.assert_array_equal(got, want)
 
 
+def test_update_with_new_rows_equals_oracle(oracle):
+    """Inserts that bring new mixture samples (the stream-update
+    configuration's inserts; the reference can only copy rows): the counts
+    equal the oracle's exact restatement, and afterwards the handle holds
+    the data of the last compaction (kNN over it equals brute force)."""
+    rows = _data(2, 3000, 12, 21)
+    flags, ids = G.update_stream_new_rows(3000, 1500, seed=22, max_in_size=10)
+    n_new = int((flags == 0).sum())
+    new_rows = G.gmm_rows(n_new, 12, 6, 0.3, seed=23)
+    r = float(np.float32(G.quantile_radius(2, 0.01, 30000, 24, rows=rows)))
+    want = oracle.update_run_rows(oracle.Dataset(2, rows), 10, flags, ids, new_rows, r)
+    plan = gts.update_plan(3000, flags, ids, 10, n_new=n_new)
+    with gts.Index(rows, 2, max_h=3, max_in_size=10) as idx:
+        got, ts, tu = idx.update_run_rows(flags, ids, new_rows, r)
+        np.testing.assert_array_equal(got, want)
+        final = np.concatenate([rows, new_rows])[plan["final_rows"]]
+        assert idx.info["num"] == len(final)
+        q = np.arange(0, len(final), 37, dtype=np.int32)
+        np.testing.assert_array_equal(idx.knn(q, 5), oracle.knn_brute(oracle.Dataset(2, final), q, 5)[0])
+
+
 # ------------------------------------------------------------- edge cases
 
 def test_k_larger_than_n_and_self():

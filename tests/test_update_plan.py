@@ -73,3 +73,21 @@ def test_plan_rejects_bad_ids():
         gts.update_plan(5, np.array([2], np.int32), np.array([-1], np.int32), 10)
     with pytest.raises(gts.GtsError):
         gts.update_plan(5, np.array([3], np.int32), np.array([0], np.int32), 10)
+
+
+def test_plan_with_new_rows_equals_the_oracle(oracle):
+    """Inserts that bring new rows: the entries of the host pass, counted by
+    brute force over the data rows followed by the new rows, give the
+    oracle's counts of the same stream."""
+    rows = G.gmm_rows(240, 6, 5, 0.4, seed=8)
+    flags, ids = G.update_stream_new_rows(240, 900, seed=9, max_in_size=7)
+    n_new = int((flags == 0).sum())
+    new_rows = G.gmm_rows(n_new, 6, 5, 0.4, seed=10)
+    r = float(np.float32(G.quantile_radius(2, 0.05, 20000, 11, rows=rows)))
+    plan = gts.update_plan(240, flags, ids, 7, n_new=n_new)
+    assert plan["ent_src"][240:].tolist() == list(range(240, 240 + n_new))
+    both = oracle.Dataset(2, np.concatenate([rows, new_rows]))
+    want = oracle.update_run_rows(oracle.Dataset(2, rows), 7, flags, ids, new_rows, r)
+    np.testing.assert_array_equal(_counts_from_plan(oracle, both, plan, r), want)
+    # the final data holds data rows and new rows
+    assert plan["final_rows"].max() >= 240
