@@ -781,9 +781,18 @@ def run_gts_update(args, w, world, rank, dev, stream):
 
     import gts_b200 as gts
     from gts_b200 import datagen as G
-    rows, _ = make_data(w, args.seed)
+    if args.new_rows:
+        # inserts bring new samples of the same mixture: the data rows are the
+        # first n of one mixture draw, the inserted rows the rest
+        flags, ids = G.update_stream_new_rows(w["n"], args.ops, args.seed + 3000, 10)
+        n_new = int((flags == 0).sum())
+        both = G.gmm_rows(w["n"] + n_new, w["dim"], w["comps"], w["sigma"], seed=args.seed)
+        rows, new_rows = both[:w["n"]], both[w["n"]:]
+    else:
+        rows, _ = make_data(w, args.seed)
+        flags, ids = G.update_stream(w["n"], args.ops, args.seed + 3000, 10)
+        new_rows = None
     r = resolve_param("update", w["batches"][0][1], w, rows, args.seed)
-    flags, ids = G.update_stream(w["n"], args.ops, args.seed + 3000, 10)
     params = gts.Params(max_h=w["max_h"], max_in_size=10)
     d_rows = torch.from_numpy(rows).to(dev)
     torch.cuda.synchronize()
@@ -804,7 +813,10 @@ def run_gts_update(args, w, world, rank, dev, stream):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         t0 = time.perf_counter()
-        c, ts, tu = idx.update_run(flags, ids, r)
+        if new_rows is not None:
+            c, ts, tu = idx.update_run_rows(flags, ids, new_rows, r)
+        else:
+            c, ts, tu = idx.update_run(flags, ids, r)
         b.record(stream)
         torch.cuda.synchronize()
         wall_call = time.perf_counter() - t0
@@ -829,13 +841,28 @@ def run_gts_update(args, w, world, rank, dev, stream):
             "build_s": statistics.mean(builds), "query_ops": int((flags == 2).sum()),
             "search_s": statistics.mean(search_s), "update_s": statistics.mean(update_s),
             "e2e": {"value": value, "unit": "ops/s",
-                    "h2d_bytes_per_step": int(flags.nbytes + ids.nbytes),
+                    "h2d_bytes_per_step": int(flags.nbytes + ids.nbytes + (new_rows.nbytes if new_rows is not None else 0)),
                     "d2h_bytes_per_step": int(counts.nbytes),
                     "note": "gts_update_run takes host buffers: the timed call includes their copies"},
             "gpu_launches": launches // max(1, args.steps), "clocks": clock_summary}
-    # the reference's answers on the stream's prefix, where saved
-    path = ref_result_path(args, w)
-    if os.path.exists(path):
+    if new_rows is not None:
+        # the reference cannot insert new rows: the oracle's exact
+        # restatement checks a prefix of the stream
+        from oracle import oracle as O
+        pre = min(args.ops, args.oracle_ops)
+        nq_pre = int((flags[:pre] == 2).sum())
+        t0 = time.perf_counter()
+        want = O.update_run_rows(O.Dataset(2, rows), 10, flags[:pre], ids[:pre], new_rows, r)
+        line["agrees_with_oracle"] = {"ops": pre, "checked": nq_pre,
+                                      "agrees": bool(np.array_equal(counts[:nq_pre], want)),
+                                      "oracle_s": time.perf_counter() - t0}
+        line["config"]["inserts"] = "new samples of the same mixture (gts_update_run_rows)"
+        path = None
+    else:
+        path = ref_result_path(args, w)
+    if path is None:
+        pass
+    elif os.path.exists(path):
         ref = np.load(path)
         vals = ref["val0"]
         line["agrees_with_reference"] = {"checked": len(vals), "identical": int((counts[:len(vals)] == vals).sum()),
@@ -905,6 +932,10 @@ def parse_args(argv=None):
                     help="cfg2 only: k uniform over {1, 8, 32, 64} per query (one batch per k per step)")
     ap.add_argument("--ops", type=int, default=1_000_000, help="cfg4: operations in the stream")
     ap.add_argument("--ref-ops", type=int, default=2000, help="cfg4: operations the reference arm runs")
+    ap.add_argument("--new-rows", action="store_true",
+                    help="cfg4: inserts bring new mixture samples (the reference can only copy rows; "
+                         "checked against the oracle on --oracle-ops operations)")
+    ap.add_argument("--oracle-ops", type=int, default=400)
     ap.add_argument("--ref-queries", type=int, default=None,
                     help="queries per batch the reference arm runs (default: per workload)")
     ap.add_argument("--ref-timeout", type=int, default=3000)
