@@ -680,7 +680,8 @@ constexpr uint32_t kStagedUnused = 0xffffffffu;
 //
 // Per item (a tile and up to a.item of its needed blocks), with gi counting
 // blocks over the CTA's life (barrier phases follow it):
-//   producer:  copy A; copy blocks 0..2 into stages gi%3; for each block:
+//   producer:  copy A (unless this CTA's previous item had the same tile);
+//              copy blocks 0..2 into stages gi%3; for each block:
 //              wait its copy, wait the epilogue of block gi-2 (frees TMEM
 //              accumulator gi%2 and stage (gi-2)%3 = (gi+1)%3), MMA chain into
 //              accumulator gi%2, commit, copy block gi+1 into the freed stage.
@@ -768,12 +769,25 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
     long long gunit = 0, u_iss = -1, u_wait = -1, u_mma = -1, t_iss = -1;
     unsigned long long blocks_done = 0, appended = 0;
 
+    // guided self-scheduling (thread 0): a CTA claims a run of consecutive
+    // items, about half the remaining items over twice the CTAs (one item at
+    // the end); consecutive items mostly belong to one tile, whose query
+    // operand then stays in shared memory
+    int c_next = 0, c_end = 0;
+    // producer lane 0: the tile whose query operand is in shared memory
+    int a_tile = -1;
     for (;;) {
         if (t == 0) {
-            const int it = atomicAdd(a.item_counter, 1);
+            const int nfull = a.n_items[0], total = nfull + a.n_items[1];
+            if (c_next >= c_end) {
+                const int done = *(volatile const int *)a.item_counter;
+                const int chunk = max(1, (total - done) / (2 * (int)gridDim.x));
+                c_next = atomicAdd(a.item_counter, chunk);
+                c_end = min(c_next + chunk, total);
+            }
+            const int it = c_next++;
             int tile = -1, nblk = 0;
-            const int nfull = a.n_items[0];
-            if (it < nfull + a.n_items[1]) {
+            if (it < total) {
                 const int2 e = it < nfull ? a.items[it] : a.items[a.items_cap - 1 - (it - nfull)];
                 tile = e.x;
                 nblk = min(a.item, min(a.bcnt[tile], a.nbcap) - e.y);
@@ -805,15 +819,24 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                              (uint32_t)kFChunkBytes, &ctl.cfull[s]);
                     u_iss = gu;
                 };
-                mbar_arrive_expect_tx(&ctl.afull, fs.arec_bytes);
-                bulk_g2s(base, a.arec + (size_t)tile * fs.arec_bytes, fs.arec_bytes, &ctl.afull);
-                a_iss++;
+                // the query operand, unless this tile's is in shared memory already
+                const bool need_a = tile != a_tile;
+                if (need_a) {
+                    mbar_arrive_expect_tx(&ctl.afull, fs.arec_bytes);
+                    bulk_g2s(base, a.arec + (size_t)tile * fs.arec_bytes, fs.arec_bytes, &ctl.afull);
+                    a_iss++;
+                }
                 // chunk stages are free at an item start (the CTA synchronised
                 // after every MMA of the last item was consumed)
                 for (int u = 0; u < SC && u < total; u++) issue_chunk(u);
                 int err = 0;
-                if (!mbar_wait(&ctl.afull, (uint32_t)(a_wait & 1), kFWait)) err = 1;
-                else a_wait++;
+                if (need_a) {
+                    if (!mbar_wait(&ctl.afull, (uint32_t)(a_wait & 1), kFWait)) err = 1;
+                    else {
+                        a_wait++;
+                        a_tile = tile;
+                    }
+                }
                 const uint64_t dah = smem_desc_sw128(a_hi_s, 1024), dal = smem_desc_sw128(a_lo_s, 1024);
                 for (int j = 0; j < nblk && !err; j++) {
                     const long long gi = gblk + j;
@@ -880,14 +903,22 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                              &ctl.full[s]);
                     c_iss = gi;
                 };
-                mbar_arrive_expect_tx(&ctl.afull, fs.arec_bytes);
-                bulk_g2s(base, a.arec + (size_t)tile * fs.arec_bytes, fs.arec_bytes, &ctl.afull);
-                a_iss++;
+                const bool need_a = tile != a_tile;
+                if (need_a) {
+                    mbar_arrive_expect_tx(&ctl.afull, fs.arec_bytes);
+                    bulk_g2s(base, a.arec + (size_t)tile * fs.arec_bytes, fs.arec_bytes, &ctl.afull);
+                    a_iss++;
+                }
                 // stages are free at an item start (the CTA synchronised)
                 for (int j = 0; j < 2 && j < nblk; j++) issue_copy(gblk + j);
                 int err = 0;
-                if (!mbar_wait(&ctl.afull, (uint32_t)(a_wait & 1), kFWait)) err = 1;
-                else a_wait++;
+                if (need_a) {
+                    if (!mbar_wait(&ctl.afull, (uint32_t)(a_wait & 1), kFWait)) err = 1;
+                    else {
+                        a_wait++;
+                        a_tile = tile;
+                    }
+                }
                 // operand descriptors: the start-address field (address >> 4,
                 // 14 bits; shared memory is below 256 KB) advances by adding
                 const uint64_t dah = smem_desc_sw128(a_hi_s, 1024), dal = smem_desc_sw128(a_lo_s, 1024);
