@@ -80,6 +80,7 @@ struct gts_index {
     int *mlp_piv = nullptr;
     int mlp_npiv = 0;
     float mlp_ymu = 0.f, mlp_ysig = 1.f, mlp_widen = 1.f;
+    float mlp_widen_at[65] = {};   // per trained k (0: none; the global factor serves)
     bool mlp_ready = false;
 
     gts::DevTree dev() const;

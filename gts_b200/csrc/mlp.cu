@@ -301,12 +301,21 @@ int mlp_features(gts_index *idx, const int *d_qids, int qnum, const int *d_ks, i
 
 // Predicted squared radius bounds (as int bits) for the fast filter's seed:
 // features, the forward pass and the seed in one kernel, no scratch.
+// The widening for k: that of the smallest trained k >= k with enough
+// held-out samples, else the global one.
+static float widen_for(const gts_index *idx, int k)
+{
+    for (int kv = std::max(k, 0); kv <= 64; kv++)
+        if (idx->mlp_widen_at[kv] > 0.f) return idx->mlp_widen_at[kv];
+    return idx->mlp_widen;
+}
+
 int mlp_seed(gts_index *idx, const int *d_qids, int qnum, int k, int *d_r2_bits, cudaStream_t st)
 {
     if (qnum <= 0) return GTS_OK;
     k_mlp_infer<<<(qnum + kInferQ - 1) / kInferQ, kMH, 0, st>>>(
         idx->rows, idx->dim, d_qids, qnum, idx->mlp_piv, idx->mlp_npiv, k, idx->mlp_P, idx->mlp_norm,
-        idx->mlp_norm + kMIn, idx->mlp_ymu, idx->mlp_ysig, idx->mlp_widen, d_r2_bits);
+        idx->mlp_norm + kMIn, idx->mlp_ymu, idx->mlp_ysig, widen_for(idx, k), d_r2_bits);
     idx->kernel_launches++;
     GTS_CUDA_TRY(cudaGetLastError());
     return GTS_OK;
@@ -478,6 +487,21 @@ int mlp_train(gts_index *idx, int n_train, int k_max, int epochs, unsigned seed,
         float d = (T[n_fit + i] - yv[i]) * ysig;
         under[i] = d;
         se += (double)d * d;
+    }
+    // per trained k, the 99.5th percentile of its own held-out
+    // under-predictions (a class with fewer than 400 samples keeps the
+    // global factor): a k whose radius the network predicts well is widened
+    // less, so its seeds stay tighter for the same ~0.5% of re-answers
+    {
+        std::vector<std::vector<float>> byk(65);
+        for (int i = 0; i < n_val; i++) byk[ks[n_fit + i]].push_back(under[i]);
+        for (int kv = 0; kv <= 64; kv++) {
+            idx->mlp_widen_at[kv] = 0.f;
+            if (byk[kv].size() < 400) continue;
+            std::sort(byk[kv].begin(), byk[kv].end());
+            const float qk = byk[kv][(size_t)(0.995 * (byk[kv].size() - 1))];
+            idx->mlp_widen_at[kv] = std::exp(std::max(qk, 0.f)) * 1.001f;
+        }
     }
     std::sort(under.begin(), under.end());
     float q = under[(size_t)(0.995 * (n_val - 1))];   // 99.5th percentile: ~0.5% of queries rerun

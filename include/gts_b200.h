@@ -288,7 +288,9 @@ int gts_range_ids(gts_index *idx, const int *qids, int qnum, float r, int *count
  * search; training runs on the device (forward, backward and Adam kernels).
  * Afterwards GTS_FORM_FAST searches may start from the predicted radius
  * (the autotuner decides per k; gts_fast_config), widened by the 99.5th
- * percentile of the held-out under-predictions, and re-answer any query
+ * percentile of the held-out under-predictions of that k (of all k where a
+ * k has fewer than 400 held-out samples; *widen reports the all-k factor),
+ * and re-answer any query
  * whose radius held fewer than k objects -- results stay exact.
  * val_rmse_log: RMS error of log(radius) on the held-out 10%; widen: factor
  * applied to predictions (both nullable).  A rebuild discards the model. */
