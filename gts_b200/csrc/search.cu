@@ -48,6 +48,7 @@ constexpr int kMaxK = 256;
 constexpr int kCandCap = kLeafObjCap + kMaxK;
 constexpr int kSortCap = 2048;        // next power of two >= kCandCap
 constexpr int kMaxDimSmem = 1024;
+constexpr int kLaneRowDim = 8;        // up to this dimension a lane filters a whole row
 
 enum SearchMode { kModeKnn = 0, kModeRangeCount = 1, kModeRangeIds = 2, kModeRangeTimed = 3 };
 
@@ -355,7 +356,7 @@ __device__ void compact_candidates(SearchSmem &s, int k)
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT) k_search(SearchArgs a)
+__global__ void __launch_bounds__(NT, 1) k_search(SearchArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SearchSmem &s = *reinterpret_cast<SearchSmem *>(smem_raw);
@@ -527,7 +528,37 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a)
 
             // ---- leaves: filter every object, collect those needing exact values
             if (nleaf > 0) {
-                if (warp_filter) {
+                if (warp_filter && t.dim <= kLaneRowDim) {
+                    // few dimensions: one lane per row, 32 rows per warp step
+                    // (the value bounds hold for any summation order)
+                    const int nl = s.nleaf;
+                    for (int o = warp * 32 + lane; o - lane < nobj; o += NT) {
+                        if (o >= nobj) continue;
+                        const int li = leaf_of(s.leaf_pre, nl, o);
+                        const int pos = t.node_lid[s.bleaf[li]] + s.bleaf_off[li] + (o - s.leaf_pre[li]);
+                        const int id = t.id_list[pos];
+                        if (is_deleted(a.deleted, id)) continue;
+                        const float *row = t.trows + (size_t)pos * t.dim;
+                        float v = 0.f;
+                        for (int j = 0; j < t.dim; j++) {
+                            const float d0 = __ldg(row + j) - qrow[j];
+                            if (t.metric == kL2) v = fmaf(d0, d0, v);
+                            else if (t.metric == kL1) v += fabsf(d0);
+                            else v = fmaxf(v, fabsf(d0));
+                        }
+                        float lo, hi;
+                        value_bounds_f(t.metric, t.dim, v, lo, hi);
+                        if (id == qid) lo = hi = 0.f;
+                        if (knn) {
+                            if ((double)lo <= s.R) s.cpos[atomicAdd(&s.ncpos, 1)] = pos;
+                        } else if (count_only && (double)hi < (double)a.r * (1.0 - 2.4e-7)) {
+                            if (timed) add_timed(a, s, id);
+                            else atomicAdd(&s.cnt, 1);
+                        } else if ((double)lo <= (double)a.r * (1.0 + 2.4e-7)) {
+                            s.cpos[atomicAdd(&s.ncpos, 1)] = pos;
+                        }
+                    }
+                } else if (warp_filter) {
                     // kRows rows per warp step: their loads are in flight
                     // together.  Lane u < kRows finds row u's leaf (binary
                     // search of the step's leaf prefix) and, after the
