@@ -636,7 +636,25 @@ __global__ void __launch_bounds__(NT, 1) k_search(SearchArgs a)
 
             // ---- internal nodes: pivot distance bounds, then ring pruning of children
             if (nint > 0) {
-                if (warp_filter) {
+                if (warp_filter && t.dim <= kLaneRowDim) {
+                    // few dimensions: one thread per pivot
+                    for (int b = tid; b < nint; b += NT) {
+                        const int piv = t.node_pivot[s.bint[b]];
+                        const float *row = t.rows + (size_t)piv * t.dim;
+                        float v = 0.f;
+                        for (int j = 0; j < t.dim; j++) {
+                            const float d0 = __ldg(row + j) - qrow[j];
+                            if (t.metric == kL2) v = fmaf(d0, d0, v);
+                            else if (t.metric == kL1) v += fabsf(d0);
+                            else v = fmaxf(v, fabsf(d0));
+                        }
+                        double lo, hi;
+                        value_bounds(t.metric, t.dim, v, lo, hi);
+                        if (piv == qid) lo = hi = 0.0;
+                        s.bdq_lo[b] = (float)lo;
+                        s.bdq_hi[b] = (float)hi;
+                    }
+                } else if (warp_filter) {
                     for (int b = warp; b < nint; b += (NT / 32)) {
                         int piv = t.node_pivot[s.bint[b]];
                         float v = warp_row_value(t.rows + (size_t)piv * t.dim, qrow, t.dim, t.metric, lane);
