@@ -313,9 +313,10 @@ def run_reference(args):
             G.write_queries(qpath, qids[sub])
             out = os.path.join(tmp, f"res{bi}.txt")
             code, param = ("0", str(int(p))) if op == "knn" else ("1", repr(float(p)))
+            dump = os.path.join(tmp, f"res{bi}.bin")
             cmd = [drv, dpath, qpath, code, param, out, "--order", "10", "--max-size", "20",
                    "--max-h", str(w["max_h"]), "--budget-gb", str(REF_BUDGET_GB[op]),
-                   "--repeat", str(repeat)]
+                   "--repeat", str(repeat), "--dump-res", dump]
             t0 = time.time()
             pr = subprocess.run(cmd, capture_output=True, text=True, timeout=args.ref_timeout)
             wall += time.time() - t0
@@ -330,10 +331,14 @@ def run_reference(args):
             t_total += t
             nq_total += len(sub)
             build_s = info["build_s"]
-            vals = open(out).read().split("\n")[2].split()
+            # the reference's res / res_dis arrays as they are in memory (the
+            # result file prints them with %f, 6 decimals)
             saved[f"pos{bi}"] = sub
-            saved[f"val{bi}"] = (np.array([int(v) for v in vals], np.int32) if op == "range"
-                                 else np.array([float(v) for v in vals], np.float32))
+            saved[f"val{bi}"] = np.fromfile(dump, dtype=np.int32 if op == "range" else np.float32)
+            if len(saved[f"val{bi}"]) != len(sub):
+                print(json.dumps({**base, "unavailable": f"reference result dump holds {len(saved[f'val{bi}'])} "
+                                                         f"values for {len(sub)} queries"}))
+                return 0
             per_batch.append({"op": op, ("k" if op == "knn" else "radius"): p, "queries": len(sub),
                               "queries_per_s": len(sub) / t, "search_s": t})
     value = nq_total / t_total
@@ -450,16 +455,19 @@ def cpu_baseline(w, rows, words, qids, batches, sample, got):
             "agrees_with_gpu": f"{agree}/{n}"}
 
 
-def compare_with_reference(args, w, batches, got):
+def compare_with_reference(args, w, batches, got, rows=None, words=None, qids=None):
     """Every answer the reference arm saved for this workload against ours:
     counts exactly, k-th distances exactly or within the reference's sort-code
-    quantum (a near-tie its quantised code swapped)."""
+    quantum (a near-tie its quantised code swapped).  Where they differ, the
+    oracle's exact brute force (given the data) says which side is right, on
+    up to 64 of those queries."""
     path = ref_result_path(args, w)
     if not os.path.exists(path):
         return {"checked": 0, "note": "no reference answers saved on this machine for this workload "
                                       "(run bench.py --impl reference first)"}
     ref = np.load(path)
     checked, exact, within, worst = 0, 0, 0, 0.0
+    differ = []   # (batch, op, param, query position, ours, reference's)
     for bi, (op, p, sel) in enumerate(batches):
         if f"pos{bi}" not in ref:
             continue
@@ -468,16 +476,41 @@ def compare_with_reference(args, w, batches, got):
         mine = np.array([got[bi][lookup[int(x)]] for x in pos])
         checked += len(pos)
         if op == "range":
-            exact += int((mine == val).sum())
-            within += int((mine == val).sum())
+            ok = mine == val
+            exact += int(ok.sum())
+            within += int(ok.sum())
         else:
             q = kth_quantum(len(pos))
             diff = np.abs(mine.astype(np.float64) - val.astype(np.float64))
+            ok = diff <= q
             exact += int((diff == 0).sum())
-            within += int((diff <= q).sum())
+            within += int(ok.sum())
             worst = max(worst, float(diff.max()) if len(diff) else 0.0)
-    return {"checked": checked, "identical": exact, "within_sort_code_quantum": within,
-            "max_abs_kth_diff": worst, "agrees": within == checked}
+        for j in np.nonzero(~ok)[0]:
+            differ.append((bi, op, p, int(pos[j]), mine[j], val[j]))
+    out = {"checked": checked, "identical": exact, "within_sort_code_quantum": within,
+           "max_abs_kth_diff": worst, "agrees": within == checked}
+    if differ and qids is not None and (rows is not None or words is not None):
+        out["differences_by_oracle"] = adjudicate(w, rows, words, qids, differ[:64])
+    return out
+
+
+def adjudicate(w, rows, words, qids, differ):
+    """The oracle's exact brute force on the queries where this build and the
+    reference disagree: how many of them each side answers exactly."""
+    from oracle import oracle as O
+    ds = O.Dataset(w["metric"], rows) if words is None else O.Dataset(6, strs=words[0], lens=words[1])
+    ours = theirs = 0
+    examples = []
+    for bi, op, p, qpos, mine, val in differ:
+        q = np.array([qids[qpos]], np.int32)
+        truth = (O.range_brute(ds, q, p)[0] if op == "range" else O.knn_brute(ds, q, int(p))[0][0])
+        ours += int(mine == truth)
+        theirs += int(val == truth)
+        if len(examples) < 5:
+            examples.append({"query": int(q[0]), "op": op, "param": p, "ours": mine.item(), "reference": val.item(),
+                             "exact": truth.item()})
+    return {"examined": len(differ), "ours_exact": ours, "reference_exact": theirs, "examples": examples}
 
 
 def flush_l2(torch, dev, buf):
@@ -537,7 +570,7 @@ def run_gts(args):
     prepare_s = time.perf_counter() - t0
     index_bytes = idx.info["device_bytes"]
     has_knn = any(op == "knn" for op, _, _ in batches)
-    fast_ok = w["metric"] == 2 and w["dim"] <= 128
+    fast_ok = w["metric"] == 2 and w["dim"] <= 320
     learn = None
     if form_name in ("fast", "plain-learned") and not args.no_learn and has_knn and fast_ok:
         # learned radius: exact radii of 200,000 objects from the index
@@ -693,7 +726,7 @@ def run_gts(args):
                         "queries": len(g["sel"]), "queries_per_s": len(g["sel"]) / (a.elapsed_time(b) / 1e3)})
         line["batches"] = per
     if rank == 0:
-        line["agrees_with_reference"] = compare_with_reference(args, w, batches, got)
+        line["agrees_with_reference"] = compare_with_reference(args, w, batches, got, rows, words, qids)
     if rank == 0 and world == 1 and args.cpu_sample > 0:
         line["cpu_baseline"] = cpu_baseline(w, rows, words, qids, batches, args.cpu_sample, got)
     if rank == 0:

@@ -41,6 +41,7 @@ gts::DevTree gts_index::dev() const
     t.tree_h = tree_h; t.max_node_num = max_node_num;
     t.dis_code = params.dis_code; t.infi_dis = params.infi_dis;
     t.rows = rows; t.trows = trows; t.strs = strs; t.tstrs = tstrs; t.lens = lens; t.tlens = tlens;
+    t.tsig = tsig;
     t.id_list = id_list; t.pos_of_id = pos_of_id;
     t.node_pid = node_pid; t.node_size = node_size; t.node_lid = node_lid; t.node_pivot = node_pivot;
     t.node_min_dis = node_min_dis; t.node_flags = node_flags;

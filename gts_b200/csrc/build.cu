@@ -49,6 +49,7 @@ template int dev_alloc<uint32_t>(uint32_t **, size_t, size_t *);
 template int dev_alloc<unsigned short>(unsigned short **, size_t, size_t *);
 template int dev_alloc<unsigned long long>(unsigned long long **, size_t, size_t *);
 template int dev_alloc<int4>(int4 **, size_t, size_t *);
+template int dev_alloc<uint4>(uint4 **, size_t, size_t *);
 
 // Build-time distance between two objects (by id), F64 or F32 site.
 __device__ __forceinline__ double obj_dist(const DevData &d, int a, int b, int acc)
@@ -173,6 +174,13 @@ __global__ void k_clear_level(int start, int nb, uint8_t *split)
 }
 
 // Tree-order copies of the data so that a leaf's objects are contiguous.
+// Character-class signatures of the strings in tree order (edit lower bounds).
+__global__ void k_str_sig(int n, const char *tstrs, const int *tlens, uint4 *tsig)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += (size_t)gridDim.x * blockDim.x)
+        tsig[i] = str_sig(tstrs + i * kStrStride, tlens[i]);
+}
+
 __global__ void k_permute(int n, int dim, int metric, const int *id_list, const float *rows,
                           float *trows, const char *strs, char *tstrs, const int *lens, int *tlens,
                           int *pos_of_id)
@@ -247,12 +255,12 @@ void free_tree(gts_index *idx)
     for (int &c : idx->plain_nt) c = 0;
     graph_invalidate(idx);
     idx->mlp_ready = false;   // its feature pivots belong to the old tree
-    void *ps[] = {idx->trows, idx->tstrs, idx->tlens, idx->id_list, idx->pos_of_id, idx->node_pid,
+    void *ps[] = {idx->trows, idx->tstrs, idx->tlens, idx->tsig, idx->id_list, idx->pos_of_id, idx->node_pid,
                   idx->node_size, idx->node_lid, idx->node_pivot, idx->node_min_dis,
                   idx->node_flags};
     for (void *p : ps)
         if (p) cudaFree(p);
-    idx->trows = nullptr; idx->tstrs = nullptr; idx->tlens = nullptr;
+    idx->trows = nullptr; idx->tstrs = nullptr; idx->tlens = nullptr; idx->tsig = nullptr;
     idx->id_list = nullptr; idx->pos_of_id = nullptr; idx->node_pid = nullptr;
     idx->node_size = nullptr; idx->node_lid = nullptr; idx->node_pivot = nullptr;
     idx->node_min_dis = nullptr; idx->node_flags = nullptr;
@@ -312,6 +320,7 @@ static int build_tree_impl(gts_index *idx, cudaStream_t s)
     if (idx->metric == kEdit) {
         ALLOC(idx->tstrs, (size_t)n * kStrStride);
         ALLOC(idx->tlens, n);
+        ALLOC(idx->tsig, n);
     } else {
         ALLOC(idx->trows, (size_t)n * idx->dim);
     }
@@ -377,6 +386,7 @@ static int build_tree_impl(gts_index *idx, cudaStream_t s)
     k_permute<<<grid_for(work, 256), 256, 0, s>>>(n, idx->dim, idx->metric, idx->id_list, idx->rows,
                                                   idx->trows, idx->strs, idx->tstrs, idx->lens,
                                                   idx->tlens, idx->pos_of_id);
+    if (idx->metric == kEdit) k_str_sig<<<grid_for((size_t)n, 256), 256, 0, s>>>(n, idx->tstrs, idx->tlens, idx->tsig);
     GTS_CUDA_TRY(cudaStreamSynchronize(s));
     GTS_CUDA_TRY(cudaGetLastError());
     return GTS_OK;

@@ -6,6 +6,8 @@
 //                                  leaf's objects are one contiguous span
 //   strs/tstrs char[num * 109]     strings (metric 6), id order / tree order
 //   lens/tlens int[num]
+//   tsig      uint4[num]           metric 6: the strings' character-class
+//                                  signatures in tree order (edit lower bounds)
 //   id_list   int[num]             tree position -> object id (tree.cuh:344)
 //   pos_of_id int[num]             object id -> tree position
 //   node_*    SoA over max_node_num nodes in the reference's implicit O-ary
@@ -36,6 +38,7 @@ struct DevTree {
     const float *rows, *trows;
     const char *strs, *tstrs;
     const int *lens, *tlens;
+    const uint4 *tsig;   // metric 6: character-class signature per tree position (metric.cuh)
     const int *id_list, *pos_of_id;
     const int *node_pid, *node_size, *node_lid, *node_pivot;
     const float *node_min_dis;

@@ -14,6 +14,7 @@ struct gts_index {
     float *rows = nullptr, *trows = nullptr;
     char *strs = nullptr, *tstrs = nullptr;
     int *lens = nullptr, *tlens = nullptr;
+    uint4 *tsig = nullptr;
     int *id_list = nullptr, *pos_of_id = nullptr;
     int *node_pid = nullptr, *node_size = nullptr, *node_lid = nullptr, *node_pivot = nullptr;
     float *node_min_dis = nullptr;

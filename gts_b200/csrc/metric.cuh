@@ -162,6 +162,47 @@ __device__ __forceinline__ int edit_dp(const char *__restrict__ a, int n,
 // fast filters (warp-cooperative, coalesced): FP32 with a rounding bound
 // ---------------------------------------------------------------------------
 
+// Character-class signature of a string: for each of 32 classes (a byte's
+// low five bits; a..z are classes 1..26) the count of its characters,
+// saturated at 15, four bits each.  One edit changes the counts' L1 distance
+// by at most 2 (a substitution moves one count, an insertion or deletion
+// changes one) and saturation only lowers it, so ceil(L1 / 2) of two
+// signatures, like the length difference, is a lower bound on the edit
+// distance of the strings.
+__device__ __forceinline__ uint4 str_sig(const char *__restrict__ s, int n)
+{
+    n = min(max(n, 0), kStrStride);
+    unsigned char cnt[32];
+#pragma unroll
+    for (int c = 0; c < 32; c++) cnt[c] = 0;
+    for (int i = 0; i < n; i++) {
+        const int c = (unsigned char)s[i] & 31;
+        if (cnt[c] < 15) cnt[c]++;
+    }
+    uint32_t w[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        uint32_t v = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) v |= (uint32_t)cnt[8 * k + j] << (4 * j);
+        w[k] = v;
+    }
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// max(|la - lb|, ceil(L1(sig_a, sig_b) / 2)) <= edit distance.
+__device__ __forceinline__ int edit_lower_bound(uint4 a, int la, uint4 b, int lb)
+{
+    const uint32_t x[4] = {a.x, a.y, a.z, a.w}, y[4] = {b.x, b.y, b.z, b.w};
+    unsigned l1 = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        l1 += __vsadu4(x[k] & 0x0F0F0F0Fu, y[k] & 0x0F0F0F0Fu);
+        l1 += __vsadu4((x[k] >> 4) & 0x0F0F0F0Fu, (y[k] >> 4) & 0x0F0F0F0Fu);
+    }
+    return max(abs(la - lb), (int)((l1 + 1) >> 1));
+}
+
 __device__ __forceinline__ float warp_sum(float v)
 {
 #pragma unroll

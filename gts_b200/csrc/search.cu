@@ -113,6 +113,7 @@ struct __align__(16) SearchSmem {
     uint64_t peq[256];
     char qstr[kStrStride + 3];
     int qlen;
+    uint4 qsig;   // the query string's character-class signature
     int stack_node[kStackCap];
     int stack_off[kStackCap];  // first unverified object of a leaf entry
     float stack_lb[kStackCap];
@@ -426,6 +427,10 @@ __global__ void __launch_bounds__(NT, 1) k_search(SearchArgs a)
                 for (int i = tid; i < t.dim; i += NT) s.qrow[i] = src[i];
         }
         __syncthreads();
+        if (t.metric == kEdit) {
+            if (tid == 0) s.qsig = str_sig(s.qstr, s.qlen);
+            __syncthreads();
+        }
         const float *qrow = t.dim <= kMaxDimSmem ? s.qrow : s.qsrc;
 
         // ---- traversal
@@ -597,10 +602,16 @@ __global__ void __launch_bounds__(NT, 1) k_search(SearchArgs a)
                         }
                     }
                 } else {
+                    // edit distance: objects whose length difference or
+                    // character-class bound already exceeds the bound are
+                    // out without their edit distance (metric.cuh)
+                    const bool sig = t.metric == kEdit && t.tsig;
+                    const double bnd = knn ? s.R : (double)a.r;
                     for (int o = tid; o < nobj; o += NT) {
                         const int li = leaf_of(s.leaf_pre, s.nleaf, o);
                         int pos = t.node_lid[s.bleaf[li]] + s.bleaf_off[li] + (o - s.leaf_pre[li]);
                         if (is_deleted(a.deleted, t.id_list[pos])) continue;
+                        if (sig && (double)edit_lower_bound(t.tsig[pos], t.tlens[pos], s.qsig, s.qlen) > bnd) continue;
                         int c = atomicAdd(&s.ncpos, 1);
                         s.cpos[c] = pos;
                     }

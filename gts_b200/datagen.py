@@ -127,13 +127,20 @@ def update_stream(n: int, n_ops: int, seed: int, max_in_size: int = 10,
     physical row of the current data array and appends a copy of it to the
     cache list; a delete names a logical id (live tree rows in physical
     order, then the cache list); a query names a physical row.  After
-    max_in_size inserts the data is compacted and rebuilt."""
+    max_in_size inserts the data is compacted and rebuilt.
+
+    Between two compactions only a handful of rows die (about as many
+    deletes as the max_in_size inserts), so the rows deleted since the last
+    compaction are a short sorted list: the (u+1)-th live row is u shifted
+    past every dead row at or before it.  O(deletes per compaction) per op,
+    nothing per compaction, for streams of millions of operations."""
+    import bisect
     rng = np.random.default_rng(seed)
     flags = np.empty(n_ops, dtype=np.int32)
     ids = np.empty(n_ops, dtype=np.int32)
     tree_size, ndel, in_size = n, 0, 0
-    dead = np.zeros(n, dtype=bool)      # deleted physical rows of the current array
-    fen = _Fenwick(n)
+    dead = []          # physical rows deleted since the last compaction, ascending
+    dead_set = set()
     u = rng.random(n_ops)
     for i in range(n_ops):
         live = tree_size - ndel + in_size
@@ -143,15 +150,19 @@ def update_stream(n: int, n_ops: int, seed: int, max_in_size: int = 10,
             if in_size == max_in_size:
                 tree_size = tree_size - ndel + in_size
                 ndel, in_size = 0, 0
-                dead = np.zeros(tree_size, dtype=bool)
-                fen = _Fenwick(tree_size)
+                dead, dead_set = [], set()
         elif u[i] < p_insert + p_delete and live > 1:
             lid = int(rng.integers(0, live))
             flags[i], ids[i] = 1, lid
             if lid < tree_size - ndel:
-                phys = fen.select(lid)
-                dead[phys] = True
-                fen.add(phys, -1)
+                phys = lid
+                for d in dead:
+                    if d <= phys:
+                        phys += 1
+                    else:
+                        break
+                bisect.insort(dead, phys)
+                dead_set.add(phys)
                 ndel += 1
             else:
                 in_size -= 1
@@ -160,7 +171,7 @@ def update_stream(n: int, n_ops: int, seed: int, max_in_size: int = 10,
             # always a hit (the reference allocates its result arrays by the
             # hit count and stops on a zero-byte managed allocation)
             q = int(rng.integers(0, tree_size))
-            while dead[q]:
+            while q in dead_set:
                 q = int(rng.integers(0, tree_size))
             flags[i], ids[i] = 2, q
     return flags, ids
@@ -176,36 +187,6 @@ def update_stream_new_rows(n: int, n_ops: int, seed: int, max_in_size: int = 10,
     ids = ids.copy()
     ids[ins] = np.arange(int(ins.sum()), dtype=np.int32)
     return flags, ids
-
-
-class _Fenwick:
-    """Counts of live rows; select(u) = physical index of the (u+1)-th live row."""
-
-    def __init__(self, n: int):
-        self.n = n
-        t = np.ones(n + 1, dtype=np.int64)
-        t[0] = 0
-        for i in range(1, n + 1):
-            j = i + (i & -i)
-            if j <= n:
-                t[j] += t[i]
-        self.t = t.tolist()
-        self.log = max(1, n.bit_length())
-
-    def add(self, i: int, v: int) -> None:
-        i += 1
-        while i <= self.n:
-            self.t[i] += v
-            i += i & -i
-
-    def select(self, u: int) -> int:
-        pos, rem = 0, u + 1
-        for b in range(self.log, -1, -1):
-            np_ = pos + (1 << b)
-            if np_ <= self.n and self.t[np_] < rem:
-                pos = np_
-                rem -= self.t[np_]
-        return pos
 
 
 # --------------------------------------------------------------------------
