@@ -382,7 +382,8 @@ extern "C" void gts_index_free(gts_index *idx)
     if (idx->scratch) cudaFree(idx->scratch);
     if (idx->split_buf) cudaFree(idx->split_buf);
     if (idx->io) cudaFree(idx->io);
-    if (idx->graph_exec) cudaGraphExecDestroy(idx->graph_exec);
+    for (int i = 0; i < gts_index::kGraphSlots; i++)
+        if (idx->graph_exec[i]) cudaGraphExecDestroy(idx->graph_exec[i]);
     if (idx->graph_stream) cudaStreamDestroy(idx->graph_stream);
     for (int i = 0; i < 2; i++)
         if (idx->graph_ev[i]) cudaEventDestroy(idx->graph_ev[i]);

@@ -1220,7 +1220,7 @@ constexpr int kFinB = 16;
 // the shared memory: twice the CTAs per SM to hide the row loads) runs
 // first over every query and lists the queries with more in `heavy`; the
 // full variant (CAP = kFCand) then runs over that list (`only`, *n_only of
-// them; CTAs past the count return at once).
+// them, a persistent grid walking the list).
 template <int KPM, int FINB, int CAP>
 __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ rows, int dim, int num,
                                                     const float *__restrict__ prow, int kp,
@@ -1247,9 +1247,11 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
     double(*terms)[KPM + 1] = reinterpret_cast<double(*)[KPM + 1]>(scratch);
     __shared__ int ns;
     __shared__ float kub;
-    if (only && (int)blockIdx.x >= *n_only) return;
-    const int q = only ? only[blockIdx.x] : (int)blockIdx.x;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int nwork = only ? *n_only : (int)gridDim.x;
+    for (int wi = blockIdx.x; wi < nwork; wi += gridDim.x) {
+    __syncthreads();   // the previous query's shared state is consumed
+    const int q = only ? only[wi] : wi;
     const int qid = qids[q];
     const int cnt = cand_cnt[q];
     if (cnt > CAP) {
@@ -1257,7 +1259,7 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
             if (CAP < kFCand && cnt <= kFCand) heavy[atomicAdd(n_heavy, 1)] = q;
             else overflow[atomicAdd(n_overflow, 1)] = q;
         }
-        return;
+        continue;
     }
     float R2 = __int_as_float(r2_bits[q]);
     if (cnt >= k && cnt <= 128) {
@@ -1419,32 +1421,33 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
     if (t == 0 && stats) atomicAdd(&stats[2], (unsigned long long)n);
     if (n <= 32) {
         // rank of each candidate by (distance, id) within warp 0
-        if (warp != 0) return;
-        const double d = lane < n ? cd[lane] : DBL_MAX;
-        const int id = lane < n ? cid[lane] : 0x7fffffff;
-        int rank = 0;
-        for (int j = 0; j < n; j++) {
-            const double dj = __shfl_sync(0xffffffffu, d, j);
-            const int ij = __shfl_sync(0xffffffffu, id, j);
-            rank += (dj < d) || (dj == d && ij < id);
+        if (warp == 0) {
+            const double d = lane < n ? cd[lane] : DBL_MAX;
+            const int id = lane < n ? cid[lane] : 0x7fffffff;
+            int rank = 0;
+            for (int j = 0; j < n; j++) {
+                const double dj = __shfl_sync(0xffffffffu, d, j);
+                const int ij = __shfl_sync(0xffffffffu, id, j);
+                rank += (dj < d) || (dj == d && ij < id);
+            }
+            const bool top = lane < n && rank < k;
+            const int within = __popc(__ballot_sync(0xffffffffu, top && d * d <= lim));
+            if (within < k && within < num) {
+                if (lane == 0) overflow[atomicAdd(n_overflow, 1)] = q;
+            } else {
+                if (top) {
+                    if (ids) ids[(size_t)q * k + rank] = id;
+                    if (dists) dists[(size_t)q * k + rank] = (float)d;
+                    if (rank == k - 1) kth[q] = (float)d;
+                }
+                for (int j = n + lane; j < k; j += 32) {
+                    if (ids) ids[(size_t)q * k + j] = -1;
+                    if (dists) dists[(size_t)q * k + j] = (float)infi_dis;
+                }
+                if (n < k && lane == 0) kth[q] = (float)infi_dis;
+            }
         }
-        const bool top = lane < n && rank < k;
-        const int within = __popc(__ballot_sync(0xffffffffu, top && d * d <= lim));
-        if (within < k && within < num) {
-            if (lane == 0) overflow[atomicAdd(n_overflow, 1)] = q;
-            return;
-        }
-        if (top) {
-            if (ids) ids[(size_t)q * k + rank] = id;
-            if (dists) dists[(size_t)q * k + rank] = (float)d;
-            if (rank == k - 1) kth[q] = (float)d;
-        }
-        for (int j = n + lane; j < k; j += 32) {
-            if (ids) ids[(size_t)q * k + j] = -1;
-            if (dists) dists[(size_t)q * k + j] = (float)infi_dis;
-        }
-        if (n < k && lane == 0) kth[q] = (float)infi_dis;
-        return;
+        continue;
     }
     // sorted above
     if (t == 0) {
@@ -1455,11 +1458,12 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
         ns = within < k && within < num ? -1 : 0;
     }
     __syncthreads();
-    if (ns < 0) return;
+    if (ns < 0) continue;
     for (int j = t; j < k; j += 128) {
         if (ids) ids[(size_t)q * k + j] = j < n ? cid[j] : -1;
         if (dists) dists[(size_t)q * k + j] = j < n ? (float)cd[j] : (float)infi_dis;
     }
+    }   // for wi
 }
 
 __global__ void k_fast_keys(const int *qids, int qnum, const int *pos_of, int *keys, int *vals)
@@ -1847,13 +1851,15 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 1ull);
     idx->kernel_launches++;
     // light recheck over every query, then the full one over those with more
-    // than 128 candidates
+    // than 128 candidates (a persistent grid of a few CTAs per SM walking
+    // their list)
+    const int final_grid = 4 * nsm;
     if (fs.kp <= kFResKp) {
         k_fast_final<kFResKp, kFinB, 128><<<qnum, 128, 0, st>>>(
             idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
             r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, r.heavy, r.ctr + 4, nullptr, nullptr,
             idx->d_stats);
-        k_fast_final<kFResKp, kFinB, kFCand><<<qnum, 128, 0, st>>>(
+        k_fast_final<kFResKp, kFinB, kFCand><<<std::min(qnum, final_grid), 128, 0, st>>>(
             idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
             r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, nullptr, nullptr, r.heavy, r.ctr + 4,
             idx->d_stats);
@@ -1862,7 +1868,7 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
             idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
             r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, r.heavy, r.ctr + 4, nullptr, nullptr,
             idx->d_stats);
-        k_fast_final<kFMaxKp, kFinB / 2, kFCand><<<qnum, 128, 0, st>>>(
+        k_fast_final<kFMaxKp, kFinB / 2, kFCand><<<std::min(qnum, final_grid), 128, 0, st>>>(
             idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
             r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, nullptr, nullptr, r.heavy, r.ctr + 4,
             idx->d_stats);
@@ -1942,9 +1948,12 @@ struct FastCall {
 
 void graph_invalidate(gts_index *idx)
 {
-    if (idx->graph_exec) cudaGraphExecDestroy(idx->graph_exec);
-    idx->graph_exec = nullptr;
-    for (long long &v : idx->graph_key) v = 0;
+    for (int i = 0; i < gts_index::kGraphSlots; i++) {
+        if (idx->graph_exec[i]) cudaGraphExecDestroy(idx->graph_exec[i]);
+        idx->graph_exec[i] = nullptr;
+        for (long long &v : idx->graph_key[i]) v = 0;
+        idx->graph_used[i] = 0;
+    }
 }
 
 // Queries listed in book[stage].fail (indices into parent_q) answered again:
@@ -2015,15 +2024,32 @@ static int fast_search_graph(gts_index *idx, FastCall &fc, const FastCfg &cfg, c
                               (long long)(uintptr_t)fc.region, (long long)(uintptr_t)idx->fast_recs,
                               (long long)(uintptr_t)d_qids, (long long)(uintptr_t)d_kth,
                               (long long)(uintptr_t)d_ids ^ ((long long)(uintptr_t)d_dists << 1)};
-    bool same = idx->graph_exec != nullptr;
-    for (int i = 0; i < 8 && same; i++) same = idx->graph_key[i] == key[i];
-    if (!same) {
+    constexpr int NS = gts_index::kGraphSlots;
+    int slot = -1, shape_slot = -1;
+    for (int s = 0; s < NS; s++) {
+        if (!idx->graph_exec[s]) continue;
+        bool same = true, shape = true;
+        for (int i = 0; i < 8; i++) same = same && idx->graph_key[s][i] == key[i];
+        for (int i = 0; i < 5; i++) shape = shape && idx->graph_key[s][i] == key[i];
+        if (same) slot = s;
+        else if (shape) shape_slot = s;
+    }
+    if (slot < 0) {
         // the same shape with other buffers twice in a row: launch directly
-        bool shape_same = idx->graph_exec != nullptr;
-        for (int i = 0; i < 5 && shape_same; i++) shape_same = idx->graph_key[i] == key[i];
-        if (shape_same && idx->graph_moved) return 1;
-        idx->graph_moved = shape_same;
-        graph_invalidate(idx);
+        if (shape_slot >= 0 && idx->graph_moved) return 1;
+        idx->graph_moved = shape_slot >= 0;
+        // capture into the slot of that shape, else a free or the least recently used one
+        slot = shape_slot;
+        if (slot < 0)
+            for (int s = 0; s < NS; s++)
+                if (!idx->graph_exec[s]) { slot = s; break; }
+        if (slot < 0) {
+            slot = 0;
+            for (int s = 1; s < NS; s++)
+                if (idx->graph_used[s] < idx->graph_used[slot]) slot = s;
+        }
+        if (idx->graph_exec[slot]) cudaGraphExecDestroy(idx->graph_exec[slot]);
+        idx->graph_exec[slot] = nullptr;
         const long long l0 = idx->kernel_launches;
         GTS_CUDA_TRY(cudaStreamBeginCapture(gs, cudaStreamCaptureModeRelaxed));
         int rc = fast_run_enqueue(idx, r, d_qids, qnum, k, cfg, learned, nullptr, d_kth, d_ids, d_dists,
@@ -2037,23 +2063,24 @@ static int fast_search_graph(gts_index *idx, FastCall &fc, const FastCfg &cfg, c
             cudaGetLastError();
             return rc ? rc : GTS_ERR_CUDA;
         }
-        e = cudaGraphInstantiate(&idx->graph_exec, g, 0);
+        e = cudaGraphInstantiate(&idx->graph_exec[slot], g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) {
-            idx->graph_exec = nullptr;
+            idx->graph_exec[slot] = nullptr;
             gts_set_error("filter graph instantiation failed: %s", cudaGetErrorString(e));
             return GTS_ERR_CUDA;
         }
-        for (int i = 0; i < 8; i++) idx->graph_key[i] = key[i];
+        for (int i = 0; i < 8; i++) idx->graph_key[slot][i] = key[i];
         // this library's kernels in the graph (CUB's and memsets not counted)
-        idx->graph_kernels = learned ? 13 : 12;
+        idx->graph_kernels[slot] = learned ? 13 : 12;
     } else {
         idx->graph_moved = false;
     }
+    idx->graph_used[slot] = ++idx->graph_clock;
     GTS_CUDA_TRY(cudaEventRecord(idx->graph_ev[0], st));
     GTS_CUDA_TRY(cudaStreamWaitEvent(gs, idx->graph_ev[0], 0));
-    GTS_CUDA_TRY(cudaGraphLaunch(idx->graph_exec, gs));
-    idx->kernel_launches += idx->graph_kernels;
+    GTS_CUDA_TRY(cudaGraphLaunch(idx->graph_exec[slot], gs));
+    idx->kernel_launches += idx->graph_kernels[slot];
     idx->graph_launches++;
     int n_fail = 0, *r2 = nullptr, rc;
     if ((rc = fast_run_finish(idx, r, &n_fail, &r2, timed, gs))) return rc;

@@ -63,13 +63,19 @@ struct gts_index {
     // CUDA graph of the fast form's filter pass (fast.cu), launched on the
     // handle's own stream and replayed while the batch shape stays the same
     cudaStream_t graph_stream = nullptr;
-    cudaGraphExec_t graph_exec = nullptr;
-    long long graph_key[8] = {};
+    // up to kGraphSlots captured filter passes, one per batch shape and
+    // argument buffers (batches of a few shapes in turn, such as one per k,
+    // each replay their own), least recently used replaced
+    static constexpr int kGraphSlots = 4;
+    cudaGraphExec_t graph_exec[kGraphSlots] = {};
+    long long graph_key[kGraphSlots][8] = {};
+    long long graph_used[kGraphSlots] = {};
+    long long graph_kernels[kGraphSlots] = {};   // this library's kernels in each graph
     cudaEvent_t graph_ev[2] = {nullptr, nullptr};
     bool use_graphs = true;
     long long graph_launches = 0;
-    long long graph_kernels = 0;   // this library's kernels in the captured graph
-    bool graph_moved = false;      // the last capture was for moved argument buffers
+    long long graph_clock = 0;
+    bool graph_moved = false;      // the last capture was for an existing shape with moved argument buffers
     // second stream of the filter pass: the own-block seeds run on it while
     // the query sort and tile operands run on the first (fast.cu)
     cudaStream_t side_stream = nullptr;

@@ -203,3 +203,19 @@ def test_streamed_records_at_resident_widths_equal_brute_force(oracle):
             np.testing.assert_array_equal(ids, bi, err_msg=f"k={k} cg={cg}")
             np.testing.assert_array_equal(kth, bk, err_msg=f"k={k} cg={cg}")
             np.testing.assert_array_equal(dis, bd, err_msg=f"k={k} cg={cg}")
+
+
+def test_graphs_of_alternating_batch_shapes(oracle):
+    """Batches of a few shapes in turn (one per k, as a mixed-k step runs
+    them) each replay their own captured graph and keep their answers."""
+    rows = G.gmm_rows(25000, 64, 20, 0.25, seed=121)
+    ds = oracle.Dataset(2, rows)
+    batches = [(G.query_ids(25000, 400, seed=122), 8), (G.query_ids(25000, 300, seed=123), 16),
+               (G.query_ids(25000, 200, seed=124), 33)]
+    with gts.Index(rows, 2, max_h=5) as idx:
+        want = [oracle.knn_brute(ds, q, k)[0] for q, k in batches]
+        n0 = idx.fast_graphs()
+        for _ in range(3):
+            for (q, k), w in zip(batches, want):
+                np.testing.assert_array_equal(idx.knn(q, k, form=gts.FORM_FAST), w, err_msg=f"k={k}")
+        assert idx.fast_graphs() - n0 == 9
