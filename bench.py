@@ -603,14 +603,19 @@ def run_gts(args):
         for g in groups:
             run_group(g)
 
-    if learn is not None and form_name == "fast" and args.learned_seed != "auto":
-        step()   # tunes the configuration for each k, then the seed choice is pinned
+    if form_name == "fast" and args.fast_filter != "auto":
+        idx.fast_range_variant(0 if args.fast_filter == "block" else 1)
+    pin_seed = learn is not None and form_name == "fast" and args.learned_seed != "auto"
+    if pin_seed or (form_name == "fast" and args.fast_filter != "auto"):
+        step()   # tunes the configuration for each k, then the seed choice or the filter is pinned
         torch.cuda.synchronize()
         for g in groups:
             if g["op"] == "knn":
                 c = idx.fast_config(int(g["p"]))
-                idx.set_fast_config(int(g["p"]), args.learned_seed == "on", c["col_groups"], c["item_blocks"],
-                                    c["streamed"])
+                learned = c["learned_seed"] if not pin_seed else args.learned_seed == "on"
+                blk = c["by_block"] if args.fast_filter == "auto" else args.fast_filter == "block"
+                streamed = c["streamed"] and not blk
+                idx.set_fast_config(int(g["p"]), learned, c["col_groups"], c["item_blocks"], streamed, blk)
     clocks = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         flush_l2(torch, dev, flush)
@@ -699,8 +704,13 @@ def run_gts(args):
         assert np.array_equal(x, y), "host-buffer and device-buffer paths disagree"
 
     peaks = measured_peaks_all()
+    # the filter the step ran: block-stationary (per k, as tuned; range counts
+    # at widths up to 128) or the tile filter
+    by_block = use_fast_timer and all(
+        idx.fast_config(int(g["p"]))["by_block"] if g["op"] == "knn"
+        else (idx.fast_range_variant() == 0 and w["dim"] <= 128) for g in groups)
     roofline = make_roofline(args, w, groups, stats, per_step_ms, total_ms, filter_ms, filter_launches,
-                             use_fast_timer, peaks)
+                             use_fast_timer, peaks, by_block)
     line = {"metric": metric_name(w), "value": value, "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -748,7 +758,8 @@ def autotune_record(idx, groups, fast):
     return {"threads_per_query_cta": {m: idx.plain_threads(i) for i, m in enumerate(("knn", "range"))}}
 
 
-def make_roofline(args, w, groups, stats, per_step_ms, total_ms, filter_ms, filter_launches, fast, peaks):
+def make_roofline(args, w, groups, stats, per_step_ms, total_ms, filter_ms, filter_launches, fast, peaks,
+                  by_block=False):
     # DRAM traffic of the dominant kernel per launch: the ncu capture's bytes
     # per unit (operand block for the filter, leaf object for the traversal)
     # times the units this run processed per launch
@@ -777,15 +788,36 @@ def make_roofline(args, w, groups, stats, per_step_ms, total_ms, filter_ms, filt
                 "per_query": {"leaf_objects": stats["objects"] / Q, "pivots": stats["pivots"] / Q,
                               "exact_rechecks": stats["exact"] / Q}}
     Q = sum(len(g["sel"]) for g in groups)
+    kp = (d + 63) // 64 * 64
+    per_step = max(1, filter_launches // max(1, args.steps))
+    kernel_ms = filter_ms / max(1, filter_launches)
+    per_query = {"blocks": stats["blocks"] / Q, "appended": stats["appended"] / Q,
+                 "exact_rechecks": stats["exact"] / Q,
+                 "fallback_queries": stats["fallback"], "passes": stats["passes"]}
+    if by_block:
+        # HBM: every item streams its block's record (BF16 operand rows of the
+        # 128 objects, the centre rows, w and |d|) once; a block needed by
+        # more than 32 queries is one item per 32 of them
+        items = stats["blocks"] / per_step
+        alg = stats["bytes"] / per_step
+        achieved = alg / (kernel_ms / 1e3) / 1e9
+        traffic = None
+        if "k_fast_blk" in per_unit:
+            traffic = per_unit["k_fast_blk"]["dram_bytes_per_item"] * items
+        return {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_kind": peaks["kind"],
+                "kernel": "k_fast_blk", "kernel_ms_per_launch": kernel_ms, "launches_per_step": per_step,
+                "kernel_share_of_step": filter_ms / total_ms,
+                "items_per_launch": items, "record_bytes_per_launch": alg,
+                "record_bytes_per_item": (stats["bytes"] / stats["blocks"]) if stats["blocks"] else None,
+                "per_query": per_query,
+                "block_pairs_kept": (stats["blocks"] / stats["tested"]) if stats["tested"] else None}
     # tensor pipe: every streamed block is one 128 x 144 x Kp MMA chain for
     # the BF16 high part and one for the low part of the queries, timed on
     # the device around every filter launch (CUDA events on the launching
     # stream); one step runs the filter once per batch, plus once per
     # re-answer stage when queries fail
-    kp = (d + 63) // 64 * 64
-    per_step = max(1, filter_launches // max(1, args.steps))
     flops = stats["blocks"] * 2 * 128 * 144 * kp * 2 / per_step
-    kernel_ms = filter_ms / max(1, filter_launches)
     achieved = flops / (kernel_ms / 1e3) / 1e12
     traffic = None
     if "k_fast_tile" in per_unit:
@@ -800,9 +832,7 @@ def make_roofline(args, w, groups, stats, per_step_ms, total_ms, filter_ms, filt
             "streamed_bytes_per_launch": streamed,
             "streamed_gbs": streamed / (kernel_ms / 1e3) / 1e9,
             "streamed_hbm_frac": streamed / (kernel_ms / 1e3) / 1e9 / peaks["hbm_gbs"],
-            "per_query": {"blocks": stats["blocks"] / Q, "appended": stats["appended"] / Q,
-                          "exact_rechecks": stats["exact"] / Q,
-                          "fallback_queries": stats["fallback"], "passes": stats["passes"]},
+            "per_query": per_query,
             "block_pairs_kept": (stats["blocks"] / stats["tested"]) if stats["tested"] else None}
 
 
@@ -980,6 +1010,9 @@ def parse_args(argv=None):
     ap.add_argument("--learned-seed", choices=["auto", "on", "off"], default="auto",
                     help="fast form with a trained radius: let the autotuner choose the learned seed, "
                          "or force it on / off (the other tuned settings are kept)")
+    ap.add_argument("--fast-filter", choices=["auto", "tile", "block"], default="auto",
+                    help="fast form: the autotuner's filter per k, or pin the tile or the block-stationary filter "
+                         "(range counts: the block filter where it fits unless tile)")
     ap.add_argument("--profile", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--dry-run", action="store_true", help=argparse.SUPPRESS)

@@ -283,7 +283,7 @@ class Index:
         v = [C.c_int() for _ in range(5)]
         _check(self._lib.gts_fast_config(self._h, k, *[C.byref(x) for x in v]))
         return {"tuned": bool(v[0].value), "learned_seed": bool(v[1].value), "col_groups": v[2].value,
-                "item_blocks": v[3].value, "streamed": bool(v[4].value)}
+                "item_blocks": v[3].value, "streamed": v[4].value == 1, "by_block": v[4].value == 2}
 
     def fast_graphs(self, on=None) -> int:
         """Turn the captured filter graph on/off (None: leave it); returns the
@@ -293,10 +293,19 @@ class Index:
         return n.value
 
     def set_fast_config(self, k: int, learned_seed: bool, col_groups: int, item_blocks: int = 16,
-                        streamed: bool = False):
-        """Pin the fast-form configuration for k instead of tuning it."""
+                        streamed: bool = False, by_block: bool = False):
+        """Pin the fast-form configuration for k instead of tuning it
+        (by_block: the block-stationary filter; col_groups and item_blocks
+        are then unused)."""
         _check(self._lib.gts_fast_config_set(self._h, k, int(bool(learned_seed)), col_groups, item_blocks,
-                                             int(bool(streamed))))
+                                             2 if by_block else int(bool(streamed))))
+
+    def fast_range_variant(self, variant=None) -> int:
+        """Filter of the fast range counts: 0 the block-stationary one where
+        it fits (default), 1 the tile one; None leaves it.  Returns it."""
+        cur = C.c_int()
+        _check(self._lib.gts_fast_range_variant(self._h, -1 if variant is None else int(variant), C.byref(cur)))
+        return cur.value
 
     def fast_autotune_reset(self):
         _check(self._lib.gts_fast_autotune_reset(self._h))

@@ -47,37 +47,20 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 #include "fast.cuh"
+#include "fast_blk.cuh"
 #include "sm100.cuh"
 
 namespace gts {
 
 using namespace sm100;
 
-constexpr int kFCand = 1024;          // candidate slots per query
 constexpr int kFItemMax = 32;         // blocks per filter work item at most (autotuned: 8, 16 or 32)
 constexpr int kFItemMin = 8;
 constexpr int kFChunk = 64;           // balls tested per pruning step
 constexpr int kNeedBlkY = 8;          // block-pruning CTAs per tile
 constexpr int kFMaxBatch = 32768;     // queries per filter run (bounds the candidate lists)
-constexpr long long kFWait = 1ll << 22;   // bounded mbarrier polls (each at most 1 us)
-
-// Error-bound constants.  Relative error of a q.x product out of the MMA:
-// the hi/lo split of q (2^-16), FP32 accumulation over 2 x 128 products
-// (taken as 2^-23 per add for margin), the FP32 rounding of r (2^-24).
-constexpr float kEpsC = 5e-5f;        // q.c rows:  >= 2^-16 + 2 * 256 * 2^-24
-constexpr float kEpsR = 8e-5f;        // q.r rows:  >= 2^-16 + 2 * 256 * 2^-23 + 2^-23
-
-// The accumulation part grows with the products summed (2 kp of them), so
-// above kp = 128 both constants scale by kp / 128: at kp = 320,
-// 1.25e-4 >= 2^-16 + 2 * 640 * 2^-24 and 2e-4 >= 2^-16 + 2 * 640 * 2^-23 + 2^-23.
-__host__ __device__ __forceinline__ float eps_scale(int kp) { return kp <= 128 ? 1.f : (float)kp / 128.f; }
-
-// Record tail, after the BF16 operand rows (floats): w[128], dn[128], then
-// |c|, the valid-object count (int), max |bf16(r)|, max |w|, the radius
-// max |o - c| (rounded up).
-constexpr int kTailW = 0, kTailDn = 128, kTailC = 256, kTailCnt = 257, kTailRb = 258, kTailWb = 259,
-              kTailRad = 260;
 
 __device__ __forceinline__ unsigned short f2bf(float x)
 {
@@ -373,6 +356,7 @@ struct NeedSmem {
     float q2s[kFT], qns[kFT], seeds[kFT];
     float c2s[kFChunk], cns[kFChunk], rads[kFChunk];
     unsigned int flags[2];
+    uint32_t lmask[kFChunk][4];   // per ball: the tile's lanes (queries) that need it
 };
 
 // The tile's query rows come from the FP32 copy k_fast_arec wrote in this
@@ -409,12 +393,14 @@ __host__ __device__ __forceinline__ size_t need_smem_bytes(int kp)
 // Balls c0 .. c0+63 (those below cend; with a list, balls list[0 .. cend-1]
 // and c0 = 0) against the tile: bit i of the result is set when some query
 // of the tile can reach ball i of the chunk within its seed:
-// |q - c|_lo - radius <= sqrt(seed).  256 threads: each computes
+// |q - c|_lo - radius <= sqrt(seed).  masks: also sm.lmask[i], the lanes of
+// the queries that reach ball i.  256 threads: each computes
 // 8 queries (4tq..4tq+3 and 64+4tq..64+4tq+3, so a quarter warp reads 128
 // consecutive bytes: no bank conflicts) x 4 balls of FP32 q.c, over the
 // centre dimensions need_kc(kp) at a time.
 __device__ __forceinline__ uint64_t need_chunk(const float *__restrict__ cen, const float *__restrict__ c2, const float *__restrict__ rad,
-                               int c0, int cend, const int *list, int kp, const float *Qs, float *Cs, NeedSmem &sm)
+                               int c0, int cend, const int *list, int kp, const float *Qs, float *Cs, NeedSmem &sm,
+                               bool masks = false)
 {
     const int t = threadIdx.x;
     const int kc = need_kc(kp);
@@ -427,6 +413,7 @@ __device__ __forceinline__ uint64_t need_chunk(const float *__restrict__ cen, co
         sm.rads[t] = ok ? rad[ball] : -1.f;
     }
     if (t < 2) sm.flags[t] = 0u;
+    if (masks) sm.lmask[t >> 2][t & 3] = 0u;   // 256 threads, 64 x 4 words
     const int tq = t & 15, tb = t >> 4;
     float acc[8][4];
 #pragma unroll
@@ -473,7 +460,7 @@ __device__ __forceinline__ uint64_t need_chunk(const float *__restrict__ cen, co
     for (int c = 0; c < 4; c++) {
         const int bb = tb * 4 + c;
         const float rd = sm.rads[bb];
-        bool nd = false;
+        uint32_t qb = 0;   // bit i: query i of this thread's eight reaches the ball
         if (rd >= 0.f) {
 #pragma unroll
             for (int i = 0; i < 8; i++) {
@@ -484,10 +471,16 @@ __device__ __forceinline__ uint64_t need_chunk(const float *__restrict__ cen, co
                 const float e = gam * sm.qns[l] * sm.cns[bb] + 4e-7f * (q2 + cc2) + 1e-30f;
                 const float d2lo = q2 - 2.f * acc[i][c] + cc2 - e;
                 const float lo = sqrtf(fmaxf(d2lo, 0.f)) * 0.999999f - rd;
-                nd |= lo <= 0.f || lo * lo * 0.999999f <= sd;
+                qb |= (lo <= 0.f || lo * lo * 0.999999f <= sd ? 1u : 0u) << i;
             }
         }
-        need |= (nd ? 1u : 0u) << c;
+        // lanes 4tq..4tq+3 (bits 0-3) and 64+4tq.. (bits 4-7)
+        if (masks && qb) {
+            const int sh = (4 * tq) & 31;
+            if (qb & 15u) atomicOr(&sm.lmask[bb][tq >> 3], (qb & 15u) << sh);
+            if (qb >> 4) atomicOr(&sm.lmask[bb][2 + (tq >> 3)], (qb >> 4) << sh);
+        }
+        need |= (qb ? 1u : 0u) << c;
     }
     // the 16 threads of a half-warp share their 4 balls
     need |= __shfl_xor_sync(0xffffffffu, need, 1);
@@ -527,7 +520,8 @@ __global__ void __launch_bounds__(256) k_need_blk(const float *__restrict__ qt,
                                                   FastSummary bs, const int *__restrict__ r2_bits,
                                                   const uint32_t *__restrict__ sb_mask, int nsbw,
                                                   int *__restrict__ blist, int *__restrict__ bcnt, int nbcap,
-                                                  unsigned long long *stats)
+                                                  unsigned long long *stats, uint4 *__restrict__ bmask,
+                                                  int *__restrict__ bq_cnt)
 {
     extern __shared__ __align__(16) float nsm[];
     __shared__ NeedSmem sm;
@@ -549,7 +543,7 @@ __global__ void __launch_bounds__(256) k_need_blk(const float *__restrict__ qt,
     int fill = 0, p = 0;
     int *dst = blist + (size_t)tile * nbcap;
     auto run_chunk = [&]() {
-        const uint64_t m0 = need_chunk(bs.cen, bs.c2, bs.rad, 0, fill, cblk[p], fs.kp, Qs, Cs, sm);
+        const uint64_t m0 = need_chunk(bs.cen, bs.c2, bs.rad, 0, fill, cblk[p], fs.kp, Qs, Cs, sm, bmask != nullptr);
         if (t == 0) {
             tested += (unsigned long long)fill;
             uint64_t m = m0;
@@ -559,7 +553,14 @@ __global__ void __launch_bounds__(256) k_need_blk(const float *__restrict__ qt,
                 while (m) {
                     const int i = __ffsll((long long)m) - 1;
                     m &= m - 1;
-                    if (at < nbcap) dst[at] = cblk[p][i];
+                    if (at < nbcap) {
+                        dst[at] = cblk[p][i];
+                        if (bmask) {
+                            const uint4 lm = make_uint4(sm.lmask[i][0], sm.lmask[i][1], sm.lmask[i][2], sm.lmask[i][3]);
+                            bmask[(size_t)tile * nbcap + at] = lm;
+                            atomicAdd(&bq_cnt[cblk[p][i]], __popc(lm.x) + __popc(lm.y) + __popc(lm.z) + __popc(lm.w));
+                        }
+                    }
                     at++;
                 }
             }
@@ -1520,18 +1521,27 @@ static int fast_cg(int k) { return k <= 32 ? 4 : 2; }
 
 // One configuration of the fast form: seed with the learned radius or not,
 // epilogue column groups (warps per query lane), blocks per work item,
-// records streamed in K chunks (forced above kp = kFResKp) or resident.
+// records streamed in K chunks (forced above kp = kFResKp) or resident --
+// or the block-stationary filter (blk; fast_blk.cu), which has no column
+// groups or items.
 struct FastCfg {
     bool learned;
     int cg, item;
     bool stream;
+    bool blk;
 };
 
 static int cfg_pack(const FastCfg &c)
 {
-    return 1 | (c.learned ? 2 : 0) | (c.cg << 2) | (c.item << 8) | (c.stream ? 1 << 14 : 0);
+    return 1 | (c.learned ? 2 : 0) | (c.cg << 2) | (c.item << 8) | (c.stream ? 1 << 14 : 0) | (c.blk ? 1 << 15 : 0);
 }
-static FastCfg cfg_unpack(int v) { return FastCfg{(v & 2) != 0, (v >> 2) & 7, (v >> 8) & 63, (v & (1 << 14)) != 0}; }
+static FastCfg cfg_unpack(int v)
+{
+    return FastCfg{(v & 2) != 0, (v >> 2) & 7, (v >> 8) & 63, (v & (1 << 14)) != 0, (v & (1 << 15)) != 0};
+}
+
+// Filter variant of a configuration as the ABI reports it.
+static int cfg_variant(const FastCfg &c) { return c.blk ? 2 : (c.stream ? 1 : 0); }
 
 static bool fast_tile_fits(const FastShape &fs, int cg, int k, bool stream);
 
@@ -1700,6 +1710,13 @@ struct RunBufs {
     int2 *items;
     void *cub;
     size_t cub_bytes;
+    // block-stationary filter (kp <= kFResKp): per (tile, needed block) the
+    // tile's lanes that need it, per block its pairs, the items and their records
+    uint4 *bmask;
+    int *bq_cnt, *bq_off, *bq_fill, *bq;
+    int4 *bitems;
+    unsigned char *irec;
+    int pairs_cap;
 };
 
 // Work items of a run at most: every tile's needed blocks in items of the
@@ -1709,7 +1726,8 @@ static size_t plan_items_cap(int ntiles, int nb)
     return std::max<size_t>((size_t)ntiles * ((nb + kFItemMin - 1) / kFItemMin), 1);
 }
 
-static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunBufs *b)
+// blk: also the block-stationary filter's buffers (kp <= kFResKp only).
+static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunBufs *b, bool blk)
 {
     const FastShape fs = fast_shape(idx->dim);
     const int ntiles = (qnum + kFT - 1) / kFT;
@@ -1740,6 +1758,21 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
     r.items = (int2 *)take(sizeof(int2) * std::max(itemcap, (size_t)1));
     r.cub = take(cub_bytes);
     r.cub_bytes = cub_bytes;
+    r.bmask = nullptr;
+    r.bq_cnt = r.bq_off = r.bq_fill = r.bq = nullptr;
+    r.bitems = nullptr;
+    r.irec = nullptr;
+    r.pairs_cap = 0;
+    if (blk && fast_blk_stages(fs) >= 2) {
+        r.pairs_cap = (int)std::min<long long>((long long)qnum * kBPairs, 1ll << 30);
+        r.bmask = (uint4 *)take(sizeof(uint4) * (size_t)ntiles * std::max(nb, 1));
+        r.bq_cnt = (int *)take(4 * (size_t)std::max(nb, 1));
+        r.bq_off = (int *)take(4 * (size_t)std::max(nb, 1));
+        r.bq_fill = (int *)take(4 * (size_t)std::max(nb, 1));
+        r.bq = (int *)take(4 * (size_t)r.pairs_cap);
+        r.bitems = (int4 *)take(sizeof(int4) * fast_blk_items_cap(nb, r.pairs_cap));
+        r.irec = take(fast_blk_irec_bytes(fs, nb, r.pairs_cap));
+    }
     if (b) *b = r;
     return off;
 }
@@ -1795,6 +1828,11 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
                                                  st));
     GTS_CUDA_TRY(cudaMemsetAsync(r.ctr, 0, 8 * sizeof(int), st));
     GTS_CUDA_TRY(cudaMemsetAsync(r.bcnt, 0, sizeof(int) * ntiles, st));
+    const bool blk = cfg.blk && r.bmask && fast_blk_stages(fs) >= 2;
+    if (blk) {
+        GTS_CUDA_TRY(cudaMemsetAsync(r.bq_cnt, 0, sizeof(int) * nb, st));
+        GTS_CUDA_TRY(cudaMemsetAsync(r.bq_fill, 0, sizeof(int) * nb, st));
+    }
     k_fast_arec<<<ntiles, 128, 0, st>>>(idx->rows, d_qids, r.order, qnum, idx->dim, fs, r.arec, r.qt);
     idx->kernel_launches++;
     if (ss != st) {
@@ -1811,11 +1849,14 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     // about four CTAs per SM share the needed superblocks
     const int need_y = std::max(kNeedBlkY, std::min(32, (4 * nsm + ntiles - 1) / ntiles));
     k_need_blk<<<dim3(ntiles, need_y), 256, need_smem, st>>>(r.qt, r.arec, fs, bs, r.r2, r.sb_mask, nsbw,
-                                                               r.blist, r.bcnt, nb, idx->d_stats);
+                                                               r.blist, r.bcnt, nb, idx->d_stats,
+                                                               blk ? r.bmask : nullptr, blk ? r.bq_cnt : nullptr);
     idx->kernel_launches++;
-    k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, r.bcnt, nb, cfg.item, r.items, r.ctr + 2,
-                                                  (int)plan_items_cap(ntiles, nb));
-    idx->kernel_launches++;
+    if (!blk) {
+        k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, r.bcnt, nb, cfg.item, r.items, r.ctr + 2,
+                                                      (int)plan_items_cap(ntiles, nb));
+        idx->kernel_launches++;
+    }
     GTS_CUDA_TRY(cudaGetLastError());
 
     FastTileArgs a;
@@ -1842,12 +1883,52 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     a.r2lo = 0.f;
     a.rcnt = nullptr;
     // events inside a captured graph must be external records to time it
-    if (timed)
-        GTS_CUDA_TRY(cudaEventRecordWithFlags(idx->fev[0], st, capturing ? cudaEventRecordExternal : 0));
-    if ((rc = launch_fast_tile(a, cfg.cg, nsm, st))) return rc;
-    idx->kernel_launches++;
-    if (timed)
-        GTS_CUDA_TRY(cudaEventRecordWithFlags(idx->fev[1], st, capturing ? cudaEventRecordExternal : 0));
+    if (blk) {
+        // pairs, items and item records, then the filter (the timed part)
+        FastBlkRun br;
+        br.args.recs = idx->fast_recs;
+        br.args.fs = fs;
+        br.args.cand_pos = r.cpos;
+        br.args.cand_lb = r.clb;
+        br.args.cand_ub = r.cub_;
+        br.args.cand_cnt = r.ccnt;
+        br.args.r2_bits = r.r2;
+        br.args.status = idx->d_status;
+        br.args.stats = idx->d_stats;
+        br.args.r2lo = 0.f;
+        br.args.rcnt = nullptr;
+        br.cen = bs.cen;
+        br.arec = r.arec;
+        br.blist = r.blist;
+        br.bmask = r.bmask;
+        br.bcnt = r.bcnt;
+        br.order = r.order;
+        br.bq_cnt = r.bq_cnt;
+        br.bq_off = r.bq_off;
+        br.bq_fill = r.bq_fill;
+        br.bq = r.bq;
+        br.irec = r.irec;
+        br.items = r.bitems;
+        br.n_items = r.ctr + 2;
+        br.nb = nb;
+        br.nbcap = nb;
+        br.ntiles = ntiles;
+        br.qnum = qnum;
+        br.pairs_cap = r.pairs_cap;
+        br.nsm = nsm;
+        br.range = false;
+        br.timed_begin = timed ? idx->fev[0] : nullptr;
+        br.timed_end = timed ? idx->fev[1] : nullptr;
+        br.capturing = capturing;
+        if ((rc = fast_blk_enqueue(br, st, &idx->kernel_launches))) return rc;
+    } else {
+        if (timed)
+            GTS_CUDA_TRY(cudaEventRecordWithFlags(idx->fev[0], st, capturing ? cudaEventRecordExternal : 0));
+        if ((rc = launch_fast_tile(a, cfg.cg, nsm, st))) return rc;
+        idx->kernel_launches++;
+        if (timed)
+            GTS_CUDA_TRY(cudaEventRecordWithFlags(idx->fev[1], st, capturing ? cudaEventRecordExternal : 0));
+    }
     k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 1ull);
     idx->kernel_launches++;
     // light recheck over every query, then the full one over those with more
@@ -1906,7 +1987,7 @@ static int fast_run(gts_index *idx, unsigned char *region, size_t region_bytes, 
                     int *d_fail, int *n_fail, int **r2_out, cudaStream_t st)
 {
     RunBufs r;
-    const size_t need = plan_run(idx, qnum, region, &r);
+    const size_t need = plan_run(idx, qnum, region, &r, cfg.blk);
     if (need > region_bytes) {
         gts_set_error("filter run needs %zu bytes of scratch, the region holds %zu", need, region_bytes);
         return GTS_ERR_INVALID;
@@ -2018,7 +2099,7 @@ static int fast_search_graph(gts_index *idx, FastCall &fc, const FastCfg &cfg, c
     const bool timed = idx->time_filter && idx->fev[0];
     const int first = learned ? 0 : 1;
     RunBufs r;
-    plan_run(idx, qnum, fc.region, &r);
+    plan_run(idx, qnum, fc.region, &r, cfg.blk);
     const long long key[8] = {qnum, k,
                               cfg_pack(cfg) | (learned ? 1 << 16 : 0) | (timed ? 1 << 19 : 0),
                               (long long)(uintptr_t)fc.region, (long long)(uintptr_t)idx->fast_recs,
@@ -2056,7 +2137,10 @@ static int fast_search_graph(gts_index *idx, FastCall &fc, const FastCfg &cfg, c
                                   fc.book[first].fail, timed, true, gs);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(gs, &g);
-        idx->kernel_launches = l0;   // counted at every replay instead
+        // this library's kernels in the graph (CUB's and memsets not
+        // counted), counted at every replay instead
+        const long long in_graph = idx->kernel_launches - l0;
+        idx->kernel_launches = l0;
         if (rc || e != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
             if (!rc) gts_set_error("filter graph capture failed: %s", cudaGetErrorString(e));
@@ -2071,8 +2155,7 @@ static int fast_search_graph(gts_index *idx, FastCall &fc, const FastCfg &cfg, c
             return GTS_ERR_CUDA;
         }
         for (int i = 0; i < 8; i++) idx->graph_key[slot][i] = key[i];
-        // this library's kernels in the graph (CUB's and memsets not counted)
-        idx->graph_kernels[slot] = learned ? 13 : 12;
+        idx->graph_kernels[slot] = in_graph;
     } else {
         idx->graph_moved = false;
     }
@@ -2146,30 +2229,37 @@ static int fast_autotune(gts_index *idx, FastCall &fc, int qc, const int *d_qids
     FastCfg best = fast_default_cfg(idx, k);
     float best_ms = 3.0e38f;
     int rc = GTS_OK;
-    for (int learned = 0; learned <= (idx->mlp_ready ? 1 : 0) && rc == GTS_OK; learned++)
-        for (int cg = 4; cg >= 1 && rc == GTS_OK; cg >>= 1) {
+    // candidates: per seed choice, the block-stationary filter, then the tile
+    // filter's column groups, item sizes and record forms
+    const FastShape fs = fast_shape(idx->dim);
+    std::vector<FastCfg> cands;
+    for (int learned = 0; learned <= (idx->mlp_ready ? 1 : 0); learned++) {
+        if (fast_blk_stages(fs) >= 2) cands.push_back(FastCfg{learned != 0, fast_cg(k), 16, false, true});
+        for (int cg = 4; cg >= 1; cg >>= 1) {
             if (k > 16 && cg * k > 128) continue;   // heaps: 128 cg threads x k x 2 bytes <= 32 KB
-            for (int item = 8; item <= kFItemMax && rc == GTS_OK; item *= 2)
-            for (int stream = fast_shape(idx->dim).kp > kFResKp ? 1 : 0; stream <= 1 && rc == GTS_OK; stream++) {
-                if (!fast_tile_fits(fast_shape(idx->dim), cg, k, stream != 0)) continue;
-                const FastCfg c{learned != 0, cg, item, stream != 0};
-                if ((rc = (int)cudaEventRecord(e0, st)) != 0) {
-                    rc = GTS_ERR_CUDA;
-                    break;
-                }
-                if ((rc = fast_search_cfg(idx, fc, qc, c, d_qids, qnum, k, d_kth, d_ids, d_dists, st))) break;
-                float ms = 0.f;
-                if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-                    cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
-                    rc = GTS_ERR_CUDA;
-                    break;
-                }
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    best = c;
-                }
-            }
+            for (int item = 8; item <= kFItemMax; item *= 2)
+                for (int stream = fs.kp > kFResKp ? 1 : 0; stream <= 1; stream++)
+                    if (fast_tile_fits(fs, cg, k, stream != 0))
+                        cands.push_back(FastCfg{learned != 0, cg, item, stream != 0, false});
         }
+    }
+    for (const FastCfg &c : cands) {
+        if (cudaEventRecord(e0, st) != cudaSuccess) {
+            rc = GTS_ERR_CUDA;
+            break;
+        }
+        if ((rc = fast_search_cfg(idx, fc, qc, c, d_qids, qnum, k, d_kth, d_ids, d_dists, st))) break;
+        float ms = 0.f;
+        if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            rc = GTS_ERR_CUDA;
+            break;
+        }
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc == GTS_ERR_CUDA) gts_set_error("autotune: CUDA event failed");
@@ -2215,7 +2305,7 @@ int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d
     // one scratch region for a run of at most kFMaxBatch queries (fewer when
     // the call's budget is smaller), reused by the re-answer stages, plus
     // their bookkeeping
-    auto rbytes_of = [&](int q) { return (plan_run(idx, q, nullptr, nullptr) + 255) & ~(size_t)255; };
+    auto rbytes_of = [&](int q) { return (plan_run(idx, q, nullptr, nullptr, true) + 255) & ~(size_t)255; };
     auto bbytes_of = [&](int q) { return (plan_book(q, k, nullptr, nullptr) + 255) & ~(size_t)255; };
     int qc = 0;
     if ((rc = run_queries_for_budget(idx, qnum, [&](int q) { return rbytes_of(q) + 3 * bbytes_of(q); }, &qc)))
@@ -2388,7 +2478,8 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
     if (rc) return rc;
     const FastShape fs = fast_shape(idx->dim);
     const int nb = idx->fast_nb, nsb = idx->fast_nsb, nsbw = (nsb + 31) / 32;
-    auto rbytes_of = [&](int q) { return (plan_run(idx, q, nullptr, nullptr) + 255) & ~(size_t)255; };
+    const bool blk = idx->range_variant == 0 && fast_blk_stages(fs) >= 2;
+    auto rbytes_of = [&](int q) { return (plan_run(idx, q, nullptr, nullptr, blk) + 255) & ~(size_t)255; };
     auto ib_of = [&](int q) { return ((size_t)q * sizeof(int) + 255) & ~(size_t)255; };
     int qc = 0;
     if ((rc = run_queries_for_budget(idx, qnum, [&](int q) { return rbytes_of(q) + 4 * ib_of(q); }, &qc)))
@@ -2419,7 +2510,7 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
         const int *dq = d_qids + q0;
         const int ntiles = (n + kFT - 1) / kFT;
         RunBufs rb;
-        plan_run(idx, n, region, &rb);
+        plan_run(idx, n, region, &rb, blk);
         k_fast_keys<<<(n + 255) / 256, 256, 0, st>>>(dq, n, bs.pos, rb.keys, rb.vals);
         size_t cb = rb.cub_bytes;
         GTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(rb.cub, cb, rb.keys, rb.skeys, rb.vals, rb.order, n, 0,
@@ -2427,6 +2518,10 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
         k_fast_range_init<<<(n + 255) / 256, 256, 0, st>>>(n, rb.ccnt, rb.r2, rcnt, r2hi_bits);
         GTS_CUDA_TRY(cudaMemsetAsync(rb.ctr, 0, 8 * sizeof(int), st));
         GTS_CUDA_TRY(cudaMemsetAsync(rb.bcnt, 0, sizeof(int) * ntiles, st));
+        if (blk) {
+            GTS_CUDA_TRY(cudaMemsetAsync(rb.bq_cnt, 0, sizeof(int) * nb, st));
+            GTS_CUDA_TRY(cudaMemsetAsync(rb.bq_fill, 0, sizeof(int) * nb, st));
+        }
         k_fast_arec<<<ntiles, 128, 0, st>>>(idx->rows, dq, rb.order, n, idx->dim, fs, rb.arec, rb.qt);
         const size_t need_smem = need_smem_bytes(fs.kp);
         GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_sb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
@@ -2435,9 +2530,11 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
             rb.qt, rb.arec, fs, bs, nsb, rb.r2, rb.sb_mask, nsbw);
         const int need_y = std::max(kNeedBlkY, std::min(32, (4 * nsm + ntiles - 1) / ntiles));
         k_need_blk<<<dim3(ntiles, need_y), 256, need_smem, st>>>(rb.qt, rb.arec, fs, bs, rb.r2, rb.sb_mask, nsbw,
-                                                                 rb.blist, rb.bcnt, nb, idx->d_stats);
-        k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, rb.bcnt, nb, 16, rb.items, rb.ctr + 2,
-                                                      (int)plan_items_cap(ntiles, nb));
+                                                                 rb.blist, rb.bcnt, nb, idx->d_stats,
+                                                                 blk ? rb.bmask : nullptr, blk ? rb.bq_cnt : nullptr);
+        if (!blk)
+            k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, rb.bcnt, nb, 16, rb.items, rb.ctr + 2,
+                                                          (int)plan_items_cap(ntiles, nb));
         GTS_CUDA_TRY(cudaGetLastError());
         FastTileArgs a;
         a.recs = idx->fast_recs;
@@ -2463,13 +2560,53 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
         a.r2lo = r2lo;
         a.rcnt = rcnt;
         const bool timed = idx->time_filter && idx->fev[0];
-        if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[0], st));
-        if ((rc = launch_fast_tile_ks<4, 8, true>(a, nsm, st))) return rc;
-        if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[1], st));
+        if (blk) {
+            FastBlkRun br;
+            br.args.recs = idx->fast_recs;
+            br.args.fs = fs;
+            br.args.cand_pos = rb.cpos;
+            br.args.cand_lb = rb.clb;
+            br.args.cand_ub = rb.cub_;
+            br.args.cand_cnt = rb.ccnt;
+            br.args.r2_bits = rb.r2;
+            br.args.status = idx->d_status;
+            br.args.stats = idx->d_stats;
+            br.args.r2lo = r2lo;
+            br.args.rcnt = rcnt;
+            br.cen = bs.cen;
+            br.arec = rb.arec;
+            br.blist = rb.blist;
+            br.bmask = rb.bmask;
+            br.bcnt = rb.bcnt;
+            br.order = rb.order;
+            br.bq_cnt = rb.bq_cnt;
+            br.bq_off = rb.bq_off;
+            br.bq_fill = rb.bq_fill;
+            br.bq = rb.bq;
+            br.irec = rb.irec;
+            br.items = rb.bitems;
+            br.n_items = rb.ctr + 2;
+            br.nb = nb;
+            br.nbcap = nb;
+            br.ntiles = ntiles;
+            br.qnum = n;
+            br.pairs_cap = rb.pairs_cap;
+            br.nsm = nsm;
+            br.range = true;
+            br.timed_begin = timed ? idx->fev[0] : nullptr;
+            br.timed_end = timed ? idx->fev[1] : nullptr;
+            br.capturing = false;
+            if ((rc = fast_blk_enqueue(br, st, &idx->kernel_launches))) return rc;
+            idx->kernel_launches += 7;   // keys, init, arec, need_sb, need_blk, stat, final
+        } else {
+            if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[0], st));
+            if ((rc = launch_fast_tile_ks<4, 8, true>(a, nsm, st))) return rc;
+            if (timed) GTS_CUDA_TRY(cudaEventRecord(idx->fev[1], st));
+            idx->kernel_launches += 9;   // keys, init, arec, need_sb, need_blk, items, tile, stat, final
+        }
         k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 1ull);
         k_fast_range_final<<<n, 128, 0, st>>>(idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, dq, r,
                                               rb.cpos, rb.ccnt, rcnt, d_counts + q0, fail, rb.ctr, idx->d_stats);
-        idx->kernel_launches += 9;   // keys, init, arec, need_sb, need_blk, items, tile, stat, final
         GTS_CUDA_TRY(cudaGetLastError());
         int status = 0, n_fail = 0;
         GTS_CUDA_TRY(cudaMemcpyAsync(&status, idx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -2501,7 +2638,7 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
     return GTS_OK;
 }
 
-int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *cg, int *item, int *streamed)
+int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *cg, int *item, int *variant)
 {
     if (k < 1 || k > kFMaxK) {
         gts_set_error("k must be in [1, %d], got %d", kFMaxK, k);
@@ -2513,38 +2650,57 @@ int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *
     if (learned) *learned = c.learned ? 1 : 0;
     if (cg) *cg = c.cg;
     if (item) *item = c.item;
-    if (streamed) *streamed = c.stream ? 1 : 0;
+    if (variant) *variant = cfg_variant(c);
     return GTS_OK;
 }
 
 }  // namespace gts
 
 extern "C" int gts_fast_config(const gts_index *idx, int k, int *tuned, int *learned, int *col_groups, int *item_blocks,
-                               int *streamed)
+                               int *variant)
 {
     if (!idx) {
         gts_set_error("null index");
         return GTS_ERR_INVALID;
     }
-    return gts::fast_config_get(idx, k, tuned, learned, col_groups, item_blocks, streamed);
+    return gts::fast_config_get(idx, k, tuned, learned, col_groups, item_blocks, variant);
 }
 
-extern "C" int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int item_blocks, int streamed)
+extern "C" int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int item_blocks, int variant)
 {
     if (!idx || k < 1 || k > gts::kFMaxK || (col_groups != 1 && col_groups != 2 && col_groups != 4) ||
-        col_groups * k > 128 || (item_blocks != 8 && item_blocks != 16 && item_blocks != 32)) {
+        col_groups * k > 128 || (item_blocks != 8 && item_blocks != 16 && item_blocks != 32) || variant < 0 ||
+        variant > 2) {
         gts_set_error("gts_fast_config_set: k in [1, 64], column groups 1/2/4 with groups * k <= 128, "
-                      "8/16/32 blocks per item");
+                      "8/16/32 blocks per item, filter variant 0/1/2");
         return GTS_ERR_INVALID;
     }
-    const bool stream = streamed != 0 || gts::fast_shape(idx->dim).kp > gts::kFResKp;
-    if (idx->metric == gts::kL2 && idx->dim <= gts::kFMaxKp &&
-        !gts::fast_tile_fits(gts::fast_shape(idx->dim), col_groups, k, stream)) {
+    const gts::FastShape fs = gts::fast_shape(idx->dim);
+    const bool l2 = idx->metric == gts::kL2 && idx->dim <= gts::kFMaxKp;
+    const bool blk = variant == 2;
+    if (blk && l2 && gts::fast_blk_stages(fs) < 2) {
+        gts_set_error("gts_fast_config_set: the block-stationary filter needs dim <= %d (got %d)", gts::kFResKp,
+                      idx->dim);
+        return GTS_ERR_INVALID;
+    }
+    const bool stream = !blk && (variant == 1 || fs.kp > gts::kFResKp);
+    if (!blk && l2 && !gts::fast_tile_fits(fs, col_groups, k, stream)) {
         gts_set_error("gts_fast_config_set: %d column groups at k %d do not fit the shared memory at dim %d",
                       col_groups, k, idx->dim);
         return GTS_ERR_INVALID;
     }
-    idx->fast_cfg[k] = gts::cfg_pack(gts::FastCfg{learned != 0, col_groups, item_blocks, stream});
+    idx->fast_cfg[k] = gts::cfg_pack(gts::FastCfg{learned != 0, col_groups, item_blocks, stream, blk});
+    return GTS_OK;
+}
+
+extern "C" int gts_fast_range_variant(gts_index *idx, int variant, int *current)
+{
+    if (!idx || variant < -1 || variant > 1) {
+        gts_set_error("gts_fast_range_variant: variant -1, 0 or 1");
+        return GTS_ERR_INVALID;
+    }
+    if (variant >= 0) idx->range_variant = variant;
+    if (current) *current = idx->range_variant;
     return GTS_OK;
 }
 

@@ -19,6 +19,30 @@ constexpr int kFResKp = 128;          // up to this padded dimension a block rec
 constexpr int kFChunkBytes = kFN * 128;   // one 64-wide K chunk of a block's operand rows
 constexpr int kFMaxK = 64;
 
+constexpr int kFCand = 1024;          // candidate slots per query
+constexpr long long kFWait = 1ll << 22;   // bounded mbarrier polls (each at most 1 us)
+
+// Error-bound constants.  Relative error of a q.x product out of the MMA:
+// the hi/lo split of q (2^-16), FP32 accumulation over 2 x 128 products
+// (taken as 2^-23 per add for margin), the FP32 rounding of r (2^-24).
+constexpr float kEpsC = 5e-5f;        // q.c rows:  >= 2^-16 + 2 * 256 * 2^-24
+constexpr float kEpsR = 8e-5f;        // q.r rows:  >= 2^-16 + 2 * 256 * 2^-23 + 2^-23
+
+// The accumulation part grows with the products summed (2 kp of them), so
+// above kp = 128 both constants scale by kp / 128: at kp = 320,
+// 1.25e-4 >= 2^-16 + 2 * 640 * 2^-24 and 2e-4 >= 2^-16 + 2 * 640 * 2^-23 + 2^-23.
+__host__ __device__ __forceinline__ float eps_scale(int kp) { return kp <= 128 ? 1.f : (float)kp / 128.f; }
+
+// Record tail, after the BF16 operand rows (floats): w[128], dn[128], then
+// |c|, the valid-object count (int), max |bf16(r)|, max |w|, the radius
+// max |o - c| (rounded up).
+constexpr int kTailW = 0, kTailDn = 128, kTailC = 256, kTailCnt = 257, kTailRb = 258, kTailWb = 259,
+              kTailRad = 260;
+
+// A candidate-list count at or above this marks a query the filter could not
+// list in full (the recheck then sends it to the re-answer stages).
+constexpr int kFListDropped = 1 << 30;
+
 // Block order (hierarchical k-means, fast_order.cu):
 constexpr int kOrdBranch = 16;        // k-means children per split at most
 constexpr int kOrdHalve = 1024;       // segments up to this size are halved instead

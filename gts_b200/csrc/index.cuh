@@ -42,6 +42,7 @@ struct gts_index {
     // autotuned fast-form configuration per k (fast.cu): 0 = not tuned, else
     // 1 | learned << 1 | column groups << 2 | blocks per item << 8
     int fast_cfg[65] = {};
+    int range_variant = 0;   // fast range counts: 0 the block-stationary filter where it fits, 1 the tile filter
     // autotuned threads per query CTA of the plain traversal per search mode
     // (kNN, range count, range ids; search.cu), 0 = not tuned
     int plain_nt[3] = {};
@@ -154,7 +155,7 @@ int search_knn_fast(gts_index *idx, const int *d_qids, int qnum, int k, float *d
                     float *d_dists, cudaStream_t s);
 int search_knn_plain_learned(gts_index *idx, const int *d_qids, int qnum, int k, float *d_kth, int *d_ids,
                              float *d_dists, cudaStream_t s);
-int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *cg, int *item, int *streamed);
+int fast_config_get(const gts_index *idx, int k, int *tuned, int *learned, int *cg, int *item, int *variant);
 int fast_prepare_now(gts_index *idx, cudaStream_t st, int *done);
 // Drop the captured filter graph (its device pointers or parameters changed).
 void graph_invalidate(gts_index *idx);

@@ -152,20 +152,29 @@ int gts_kernel_launches(const gts_index *idx, long long *count);
  * constants, search_v2.cuh: THREAD_NUM).  The GTS_FORM_FAST configuration
  * used for k on this index.  The first batch of at least 2048 queries with a
  * given k is run once per candidate -- learned-radius seed on or off (when a
- * model is trained), 4 / 2 / 1 epilogue warps per query lane, 8 / 16 / 32
- * blocks per work item, block records resident per stage or streamed in
- * 64-wide K chunks (*streamed; always streamed above dim 128) -- and the
+ * model is trained), and the filter: the block-stationary one (each needed
+ * block read once per run and multiplied with the queries that need it;
+ * dim <= 128), or the tile one with 4 / 2 / 1 epilogue warps per query
+ * lane, 8 / 16 / 32 blocks per work item, block records resident per stage
+ * or streamed in 64-wide K chunks (always streamed above dim 128) -- and the
  * fastest that fits the shared memory is kept (every candidate returns the
- * same exact answers).  *tuned = 0 reports the default that smaller batches
- * use.  Any output pointer may be NULL. */
+ * same exact answers).  *variant: 0 tile filter, resident records; 1 tile
+ * filter, streamed records; 2 block-stationary filter (*col_groups and
+ * *item_blocks then unused).  *tuned = 0 reports the default that smaller
+ * batches use.  Any output pointer may be NULL. */
 int gts_fast_config(const gts_index *idx, int k, int *tuned, int *learned, int *col_groups, int *item_blocks,
-                    int *streamed);
+                    int *variant);
 
 /* Pin the configuration for k (learned seed 0/1, 1/2/4 column groups with
- * groups * k <= 128, 8/16/32 blocks per item, streamed 0/1) instead of
- * tuning it; GTS_ERR_INVALID when it does not fit this index's shared
- * memory plan. */
-int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int item_blocks, int streamed);
+ * groups * k <= 128, 8/16/32 blocks per item, filter variant 0/1/2 as
+ * gts_fast_config reports it) instead of tuning it; GTS_ERR_INVALID when it
+ * does not fit this index's shared memory plan. */
+int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int item_blocks, int variant);
+
+/* The filter of GTS_FORM_FAST range counts: variant 0 the block-stationary
+ * filter where it fits (dim <= 128; the default), 1 the tile filter; -1
+ * leaves it.  *current (nullable) receives the setting. */
+int gts_fast_range_variant(gts_index *idx, int variant, int *current);
 
 /* Forget the tuned configurations (the next large batch tunes again). */
 int gts_fast_autotune_reset(gts_index *idx);
