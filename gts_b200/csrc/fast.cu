@@ -985,7 +985,8 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                 const long long gi = gblk + j;
                 const int s = (int)(gi % kFS);
                 const int blk = ctl.blk[j];
-                if (!mbar_wait(&ctl.mmad[s], (uint32_t)((gi / kFS) & 1), kFWait)) {
+                // one verdict per warp: the TMEM loads below are warp-collective
+                if (!__all_sync(0xffffffffu, mbar_wait(&ctl.mmad[s], (uint32_t)((gi / kFS) & 1), kFWait))) {
                     atomicMax(&ctl.err, 4);
                     break;
                 }

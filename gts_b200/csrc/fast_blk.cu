@@ -439,7 +439,8 @@ __global__ void __launch_bounds__(160, 1) k_fast_blk(FastBlkArgs a)
         for (int j = 0; j < n_local; j++) {
             const int s = j % S;
             const uint32_t ph = (uint32_t)((j / S) & 1);
-            if (!mbar_wait(&ctl.mmad[s], ph, kFWait)) {
+            // one verdict per warp: the TMEM loads below are warp-collective
+            if (!__all_sync(0xffffffffu, mbar_wait(&ctl.mmad[s], ph, kFWait))) {
                 atomicMax(&ctl.err, 4);
                 break;
             }
