@@ -809,6 +809,7 @@ def make_roofline(args, w, groups, stats, per_step_ms, total_ms, filter_ms, filt
                 "kernel": "k_fast_blk", "kernel_ms_per_launch": kernel_ms, "launches_per_step": per_step,
                 "kernel_share_of_step": filter_ms / total_ms,
                 "items_per_launch": items, "record_bytes_per_launch": alg,
+                "pairs_per_query": stats["queries"] / Q,
                 "record_bytes_per_item": (stats["bytes"] / stats["blocks"]) if stats["blocks"] else None,
                 "per_query": per_query,
                 "block_pairs_kept": (stats["blocks"] / stats["tested"]) if stats["tested"] else None}

@@ -1772,7 +1772,7 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
         r.bq_fill = (int *)take(4 * (size_t)std::max(nb, 1));
         r.bq = (int *)take(4 * (size_t)r.pairs_cap);
         r.bitems = (int4 *)take(sizeof(int4) * fast_blk_items_cap(nb, r.pairs_cap));
-        r.irec = take(fast_blk_irec_bytes(fs, nb, r.pairs_cap));
+        r.irec = take(fast_blk_irec_bytes(nb, r.pairs_cap));
     }
     if (b) *b = r;
     return off;

@@ -24,14 +24,13 @@
 //   k_bq_items            exclusive scan of the counts: each block's pairs
 //                         get a range, split into items of <= kBQ queries
 //   k_bq_fill             the pairs' query slots into their block's range
-//   k_bq_build            per item, a record in the filter's shared-memory
-//                         layout: per column the query's bound terms against
-//                         this block, then the queries' BF16 operand rows
-//                         (hi, lo), swizzled for their row in the item
-//   k_fast_blk            persistent CTAs stream (block record, item record)
-//                         pairs through shared memory, MMA, and list every
-//                         object whose lower bound is within the query's
-//                         bound (range: count the certain ones)
+//   k_bq_build            per item, its header: per column the query's bound
+//                         terms against this block and its tile slot
+//   k_fast_blk            persistent CTAs stream (block record, item header)
+//                         pairs through shared memory, gather the item's
+//                         query rows from the tile records (L2), MMA, and
+//                         list every object whose lower bound is within the
+//                         query's bound (range: count the certain ones)
 // Pairs beyond the run's capacity (qnum * kBPairs) are not listed; their
 // queries are marked (kFListDropped) and answered again by the re-answer
 // stages, so the answers stay exact.
@@ -61,12 +60,14 @@ struct __align__(16) BlkCol {
     float A, RT, T, eb;
     float RLT;
     int qi;       // query index in the run; -1: unused column or ball beyond the bound
-    int pad0, pad1;
+    int slot;     // the query's tile slot (tile * 128 + lane)
+    int pad;
 };
 static_assert(sizeof(BlkCol) * kBQ == kBHead, "item header size");
 
 struct __align__(16) BlkCtl {
-    uint64_t full[kBSMax];    // record + item record landed in stage s
+    uint64_t full[kBSMax];    // record + item header landed in stage s
+    uint64_t gfull[kBSMax];   // the item's query rows gathered into stage s
     uint64_t mmad[kBSMax];    // MMA chain into accumulator s done
     uint64_t rfree[kBSMax];   // epilogue read the record tail of stage s (one arrive per warp)
     uint64_t efree[kBSMax];   // epilogue of accumulator s done (one arrive per warp)
@@ -78,8 +79,11 @@ struct __align__(16) BlkCtl {
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src)
 {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
+// this thread's completed generic-proxy shared-memory writes, visible to the
+// async proxy (the tensor core's operand reads)
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
@@ -98,7 +102,7 @@ __device__ __forceinline__ float bfh(uint32_t v) { return __uint_as_float(v & 0x
 // index); an item's record sits at item * kBHead + first pair * 4 kp bytes.
 __global__ void __launch_bounds__(1024) k_bq_items(int nb, const int *__restrict__ cnt, int *__restrict__ off,
                                                    int4 *__restrict__ items, int *__restrict__ n_items,
-                                                   int pairs_cap)
+                                                   int pairs_cap, unsigned long long *stats)
 {
     __shared__ int wsum[2][32];
     __shared__ int carry[2];
@@ -161,7 +165,10 @@ __global__ void __launch_bounds__(1024) k_bq_items(int nb, const int *__restrict
         }
         __syncthreads();
     }
-    if (t == 0) *n_items = carry[1];
+    if (t == 0) {
+        *n_items = carry[1];
+        if (stats) atomicAdd(&stats[3], (unsigned long long)carry[0]);   // pairs, before the cap
+    }
 }
 
 // One CTA per tile: each (tile, needed block) entry's queries into the
@@ -199,10 +206,11 @@ __global__ void __launch_bounds__(256) k_bq_fill(const int *__restrict__ blist, 
     }
 }
 
-// One warp per item: the item record.  Header: kBQ columns (BlkCol); then
-// for part (hi, lo) and K chunk c, the item's nq rows of 128 bytes, row n
-// holding the query's 64 BF16 values with 16-byte unit u at u ^ (n % 8)
-// (the 128-byte swizzle of a row n of the filter's operand tile).
+// One warp per item: the item's header, kBQ columns (BlkCol) of the bound
+// terms of its queries against its block.  q.c comes from the query's BF16
+// hi + lo operand rows in its tile record (what the MMA multiplies) and the
+// block's FP32 centre: lane l holds one 16-byte unit (8 dimensions) of the
+// hi or lo rows.
 __global__ void __launch_bounds__(256) k_bq_build(const int4 *__restrict__ items, const int *__restrict__ n_items,
                                                   const int *__restrict__ bq, const unsigned char *__restrict__ arec,
                                                   const unsigned char *__restrict__ recs, const float *__restrict__ cen,
@@ -218,9 +226,7 @@ __global__ void __launch_bounds__(256) k_bq_build(const int4 *__restrict__ items
     for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < nit; it += (gridDim.x * blockDim.x) >> 5) {
         const int4 d = items[it];
         const int blk = d.x, p0 = d.y, nq = d.z;
-        unsigned char *out = irec + (size_t)it * kBHead + (size_t)p0 * 4 * fs.kp;
-        BlkCol *cols = reinterpret_cast<BlkCol *>(out);
-        const uint32_t rows_bytes = (uint32_t)nq * 128u;
+        BlkCol *cols = reinterpret_cast<BlkCol *>(irec + (size_t)it * kBHead);
         // the centre values of this lane's eight dimensions
         float cv[8];
         {
@@ -240,8 +246,6 @@ __global__ void __launch_bounds__(256) k_bq_build(const int4 *__restrict__ items
                 const uint4 v = *reinterpret_cast<const uint4 *>(arec + (size_t)tile * fs.arec_bytes +
                                                                  (size_t)p * fs.atile_bytes + (size_t)c * (kFT * 128) +
                                                                  (size_t)L * 128 + ((u ^ (L & 7)) << 4));
-                *reinterpret_cast<uint4 *>(out + kBHead + (size_t)(p * nk + c) * rows_bytes + (size_t)n * 128 +
-                                           ((u ^ (n & 7)) << 4)) = v;
                 part = fmaf(bfl(v.x), cv[0], part);
                 part = fmaf(bfh(v.x), cv[1], part);
                 part = fmaf(bfl(v.y), cv[2], part);
@@ -259,7 +263,7 @@ __global__ void __launch_bounds__(256) k_bq_build(const int4 *__restrict__ items
         // filter's epilogue terms, with q.c from the sum above: FP32 over
         // at most 16 products per lane and a 5-level tree, inside kEpsC)
         float4 f0 = make_float4(0.f, 0.f, 0.f, 0.f);   // A, RT, T, eb
-        int4 f1 = make_int4(0, -1, 0, 0);               // RLT (bits), qi
+        int4 f1 = make_int4(0, -1, 0, 0);               // RLT (bits), qi, query slot
         if (lane < nq) {
             const int tile = myslot >> 7, L = myslot & 127;
             const int4 inf = *reinterpret_cast<const int4 *>(arec + (size_t)tile * fs.arec_bytes + 2 * fs.atile_bytes +
@@ -281,7 +285,7 @@ __global__ void __launch_bounds__(256) k_bq_build(const int4 *__restrict__ items
                 const float dlo = sqrtf(fmaxf(qmc2 - ec - 4e-6f * (q2 + c2), 0.f)) * 0.999999f - brad;
                 const bool skip = dlo > 0.f && dlo * dlo * 0.999999f > R2;
                 f0 = make_float4(A, R2 - T, T, eb);
-                f1 = make_int4(__float_as_int(r2lo - T - 2e-6f * q2), skip ? -1 : qi, 0, 0);
+                f1 = make_int4(__float_as_int(r2lo - T - 2e-6f * q2), skip ? -1 : qi, myslot, 0);
             }
         }
         reinterpret_cast<float4 *>(cols + lane)[0] = f0;
@@ -292,15 +296,21 @@ __global__ void __launch_bounds__(256) k_bq_build(const int4 *__restrict__ items
 // ---------------------------------------------------------------- filter
 
 // Persistent filter, one CTA per SM: 4 epilogue warps (warp w: TMEM lanes
-// and block objects 32w .. 32w + 31) and one producer warp.  CTA b takes
-// items b, b + G, b + 2G, ...  Per item j (stage s = j % S, accumulator s,
-// header slot j % 2S):
-//   producer: copy the block record and the item record (header, operand
-//             rows) into stage s with bulk copies (S - 1 items ahead; stage
-//             s is reused once the epilogue of item j - S has read its record
-//             tail and its MMAs are done), wait for them, wait for the
-//             epilogue of item j - S (frees accumulator s), then the MMA
+// and block objects 32w .. 32w + 31), one producer warp and one gather
+// warp.  CTA b takes items b, b + G, b + 2G, ...  Per item j (stage s =
+// j % S, accumulator s, header slot j % 2S):
+//   producer: copy the block record and the item header into stage s with
+//             bulk copies (S - 1 items ahead; stage s is reused once the
+//             epilogue of item j - S has read its record tail, its MMAs being
+//             done), wait for them and for the gathered query rows, wait for
+//             the epilogue of item j - S (frees accumulator s), then the MMA
 //             chain objects x queries into accumulator s, hi and lo parts.
+//   gather:   once the MMAs of item j - S are done, copy the item's query
+//             rows (hi, lo) from their tile records, which stay in L2, into
+//             the stage's operand area: 16-byte cp.async copies, row n's
+//             units re-swizzled from the tile row's position to row n's;
+//             one item behind, wait for the copies, fence them for the
+//             tensor core's proxy and arrive on gfull.
 //   epilogue: wait the MMA, read the objects' w and |d| (then the stage is
 //             free), bound every (object, column) pair, list the passing
 //             objects in their query's candidate list (one atomic per warp
@@ -308,7 +318,7 @@ __global__ void __launch_bounds__(256) k_bq_build(const int4 *__restrict__ items
 // The header of item j stays in its own slot until the epilogue of item
 // j + S - 1 starts (2S slots), so the stage can be refilled early.
 template <bool RANGE>
-__global__ void __launch_bounds__(160, 1) k_fast_blk(FastBlkArgs a)
+__global__ void __launch_bounds__(192, 1) k_fast_blk(FastBlkArgs a)
 {
     extern __shared__ __align__(1024) unsigned char bsm[];
     unsigned char *base = bsm + ((1024u - (smem_u32(bsm) & 1023u)) & 1023u);
@@ -329,6 +339,7 @@ __global__ void __launch_bounds__(160, 1) k_fast_blk(FastBlkArgs a)
     if (t == 0) {
         for (int s = 0; s < kBSMax; s++) {
             mbar_init(&ctl.full[s], 1);
+            mbar_init(&ctl.gfull[s], 1);
             mbar_init(&ctl.mmad[s], 1);
             mbar_init(&ctl.rfree[s], 4);
             mbar_init(&ctl.efree[s], 4);
@@ -365,18 +376,14 @@ __global__ void __launch_bounds__(160, 1) k_fast_blk(FastBlkArgs a)
                 cp_async_wait<kBPre - 1>();   // j + kBPre groups committed: descriptor j landed
                 const int4 d = ring[j % kBRing];
                 prefetch(j + kBPre);
-                const int blk = d.x, p0 = d.y, nq = d.z, it = d.w;
+                const int blk = d.x, nq = d.z, it = d.w;
                 ctl.blk[s] = blk;
                 ctl.ncol[s] = nq;
-                const size_t ro = (size_t)it * kBHead + (size_t)p0 * 4 * fs.kp;
-                const uint32_t rows_bytes = (uint32_t)nq * 128u;
                 unsigned char *st = base + (size_t)s * stage_bytes;
-                mbar_arrive_expect_tx(&ctl.full[s], fs.rec_bytes + (uint32_t)kBHead + 2u * fs.nk * rows_bytes);
+                mbar_arrive_expect_tx(&ctl.full[s], fs.rec_bytes + (uint32_t)kBHead);
                 bulk_g2s(st, a.recs + (size_t)blk * fs.rec_bytes, fs.rec_bytes, &ctl.full[s]);
-                bulk_g2s(heads + (size_t)(j % (2 * S)) * kBQ, a.irec + ro, (uint32_t)kBHead, &ctl.full[s]);
-                for (int pc = 0; pc < 2 * fs.nk; pc++)
-                    bulk_g2s(st + rec_pad + (uint32_t)(pc / fs.nk) * part_bytes + (uint32_t)(pc % fs.nk) * (kBQ * 128u),
-                             a.irec + ro + kBHead + (size_t)pc * rows_bytes, rows_bytes, &ctl.full[s]);
+                bulk_g2s(heads + (size_t)(j % (2 * S)) * kBQ, a.irec + (size_t)it * kBHead, (uint32_t)kBHead,
+                         &ctl.full[s]);
                 c_iss = j;
             };
             for (int j = 0; j < S - 1 && j < n_local; j++) issue(j);
@@ -394,6 +401,7 @@ __global__ void __launch_bounds__(160, 1) k_fast_blk(FastBlkArgs a)
                 }
                 if (!mbar_wait(&ctl.full[s], (uint32_t)((j / S) & 1), kFWait)) { err = 1; break; }
                 c_wait = j;
+                if (!mbar_wait(&ctl.gfull[s], (uint32_t)((j / S) & 1), kFWait)) { err = 5; break; }
                 // accumulator s: the epilogue of item j - S is done
                 if (j >= S && !mbar_wait(&ctl.efree[s], (uint32_t)(((j - S) / S) & 1), kFWait)) { err = 2; break; }
                 tc_fence_after();
@@ -430,6 +438,64 @@ __global__ void __launch_bounds__(160, 1) k_fast_blk(FastBlkArgs a)
                 atomicAdd(&a.stats[0], (unsigned long long)(c_wait + 1));
                 atomicAdd(&a.stats[1], (unsigned long long)fs.rec_bytes * (c_wait + 1));
             }
+        }
+        __syncwarp();
+    } else if (warp == 5) {
+        // gather: lane l copies one 16-byte unit (part p, K chunk c, unit u)
+        // of every query row of the item
+        const int nk = fs.nk, units = 2 * nk * 8;
+        const int p = lane / (nk * 8), c = (lane / 8) % nk, u = lane & 7;
+        const bool act = lane < units;
+        const size_t src_off = (size_t)p * fs.atile_bytes + (size_t)c * (kFT * 128);
+        const uint32_t dst_off = rec_pad + (uint32_t)p * part_bytes + (uint32_t)c * (kBQ * 128u);
+        int4 d = make_int4(0, 0, 0, 0);
+        int slot = 0;
+        if (n_local > 0) {
+            d = a.items[blockIdx.x];
+            slot = lane < d.z ? a.bq[d.y + lane] : 0;
+        }
+        bool ok = true;
+        for (int j = 0; j < n_local; j++) {
+            const int s = j % S;
+            // the operand area of stage s: free once the MMAs of item j - S are done
+            if (j >= S &&
+                !__all_sync(0xffffffffu, mbar_wait(&ctl.mmad[s], (uint32_t)(((j - S) / S) & 1), kFWait))) {
+                ok = false;
+                break;
+            }
+            if (__any_sync(0xffffffffu, *(volatile int *)&ctl.err != 0)) {
+                ok = false;
+                break;
+            }
+            unsigned char *dst = base + (size_t)s * stage_bytes + dst_off;
+            for (int n = 0; n < d.z; n++) {
+                const int sl = __shfl_sync(0xffffffffu, slot, n);
+                if (act) {
+                    const int tile = sl >> 7, L = sl & 127;
+                    cp_async16(dst + (size_t)n * 128 + ((u ^ (n & 7)) << 4),
+                               a.arec + (size_t)tile * fs.arec_bytes + src_off + (size_t)L * 128 + ((u ^ (L & 7)) << 4));
+                }
+            }
+            cp_async_commit();
+            // the next item's descriptor (its latency overlaps the wait below)
+            int4 dn = d;
+            if (j + 1 < n_local) dn = a.items[(size_t)blockIdx.x + (size_t)(j + 1) * G];
+            if (j >= 1) {   // item j - 1's rows landed: hand them to the producer
+                cp_async_wait<1>();
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&ctl.gfull[(j - 1) % S]);
+            }
+            if (j + 1 < n_local) {
+                slot = lane < dn.z ? a.bq[dn.y + lane] : 0;
+                d = dn;
+            }
+        }
+        cp_async_wait_all();
+        if (ok && n_local > 0) {
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&ctl.gfull[(n_local - 1) % S]);
         }
         __syncwarp();
     } else if (warp < 4) {
@@ -540,15 +606,12 @@ int fast_blk_stages(const FastShape &fs)
 
 size_t fast_blk_items_cap(int nb, int pairs_cap) { return (size_t)nb + (size_t)pairs_cap / kBQ + 1; }
 
-size_t fast_blk_irec_bytes(const FastShape &fs, int nb, int pairs_cap)
-{
-    return fast_blk_items_cap(nb, pairs_cap) * kBHead + (size_t)pairs_cap * 4 * fs.kp;
-}
+size_t fast_blk_irec_bytes(int nb, int pairs_cap) { return fast_blk_items_cap(nb, pairs_cap) * kBHead; }
 
 int fast_blk_enqueue(const FastBlkRun &r, cudaStream_t st, long long *launches)
 {
     const FastShape fs = r.args.fs;
-    k_bq_items<<<1, 1024, 0, st>>>(r.nb, r.bq_cnt, r.bq_off, r.items, r.n_items, r.pairs_cap);
+    k_bq_items<<<1, 1024, 0, st>>>(r.nb, r.bq_cnt, r.bq_off, r.items, r.n_items, r.pairs_cap, r.args.stats);
     k_bq_fill<<<r.ntiles, 256, 0, st>>>(r.blist, r.bmask, r.bcnt, r.nbcap, r.bq_off, r.bq_fill, r.bq, r.pairs_cap,
                                         r.order, r.qnum, r.args.cand_cnt);
     const int build_grid = (int)std::min<size_t>((fast_blk_items_cap(r.nb, r.pairs_cap) + 7) / 8, (size_t)8 * r.nsm);
@@ -557,6 +620,8 @@ int fast_blk_enqueue(const FastBlkRun &r, cudaStream_t st, long long *launches)
     FastBlkArgs a = r.args;
     a.irec = r.irec;
     a.items = r.items;
+    a.bq = r.bq;
+    a.arec = r.arec;
     a.n_items = r.n_items;
     a.nst = fast_blk_stages(fs);
     if (a.nst < 2) {
@@ -568,10 +633,10 @@ int fast_blk_enqueue(const FastBlkRun &r, cudaStream_t st, long long *launches)
     if (r.timed_begin) GTS_CUDA_TRY(cudaEventRecordWithFlags(r.timed_begin, st, rec_flags));
     if (r.range) {
         GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_blk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_fast_blk<true><<<r.nsm, 160, smem, st>>>(a);
+        k_fast_blk<true><<<r.nsm, 192, smem, st>>>(a);
     } else {
         GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_blk<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_fast_blk<false><<<r.nsm, 160, smem, st>>>(a);
+        k_fast_blk<false><<<r.nsm, 192, smem, st>>>(a);
     }
     if (r.timed_end) GTS_CUDA_TRY(cudaEventRecordWithFlags(r.timed_end, st, rec_flags));
     if (launches) *launches += 4;

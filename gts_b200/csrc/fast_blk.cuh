@@ -9,13 +9,15 @@ namespace gts {
 
 constexpr int kBQ = 32;          // queries (MMA columns) per item at most
 constexpr int kBHead = 1024;     // item header: kBQ columns of bound terms
-constexpr int kBPairs = 16;      // (query, block) pairs per query a run stores, on average at most
+constexpr int kBPairs = 64;      // (query, block) pairs per query a run stores, on average at most
 
 struct FastBlkArgs {
     const unsigned char *recs;   // block records
-    const unsigned char *irec;   // item records (k_bq_build)
+    const unsigned char *irec;   // item headers (k_bq_build), kBHead bytes each
     const int4 *items;           // (block, first pair, queries, item index)
     const int *n_items;
+    const int *bq;               // query slots of the pairs
+    const unsigned char *arec;   // tile records: the queries' operand rows
     FastShape fs;
     int nst;                     // record stages
     int *cand_pos;               // [qnum][kFCand]
@@ -40,7 +42,7 @@ struct FastBlkRun {
     const int *order;            // tile slot -> query index
     int *bq_cnt, *bq_off, *bq_fill;   // [nb] (bq_cnt counted by the pruning, bq_fill zeroed)
     int *bq;                     // [pairs_cap] query slots
-    unsigned char *irec;         // [fast_blk_irec_bytes] item records (the filter reads args.irec = irec)
+    unsigned char *irec;         // [fast_blk_irec_bytes] item headers (the filter reads args.irec = irec)
     int4 *items;                 // [fast_blk_items_cap]
     int *n_items;
     int nb, nbcap, ntiles, qnum, pairs_cap, nsm;
@@ -53,9 +55,9 @@ struct FastBlkRun {
 // (0: the form does not apply, kp above kFResKp).
 size_t fast_blk_smem(const FastShape &fs, int nst);
 int fast_blk_stages(const FastShape &fs);
-// Items and item-record bytes a run with pairs_cap pairs may need.
+// Items and item-header bytes a run with pairs_cap pairs may need.
 size_t fast_blk_items_cap(int nb, int pairs_cap);
-size_t fast_blk_irec_bytes(const FastShape &fs, int nb, int pairs_cap);
+size_t fast_blk_irec_bytes(int nb, int pairs_cap);
 // Items, pairs, item records and the filter, enqueued on st.
 int fast_blk_enqueue(const FastBlkRun &r, cudaStream_t st, long long *launches);
 
