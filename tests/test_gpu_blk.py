@@ -108,3 +108,21 @@ def test_by_block_range_counts_equal_brute_force(oracle, n, dim, comps, sigma, m
                 assert idx.fast_range_variant(variant) == variant
                 got = idx.range(q, r, form=gts.FORM_FAST)
                 np.testing.assert_array_equal(got, want, err_msg=f"r={r} variant={variant}")
+
+
+def test_by_block_many_items_per_cta_equal_tile_filter():
+    """200,000 objects and 6,000 queries: every CTA runs dozens of items, so
+    stages, accumulators and header slots are reused many times over; the
+    answers equal the tile filter's for small, middle and large k."""
+    rows = G.gmm_rows(200000, 64, 128, 0.25, seed=161)
+    q = G.query_ids(200000, 6000, seed=162)
+    with gts.Index(rows, 2, max_h=6) as idx:
+        for k in (1, 8, 64):
+            idx.set_fast_config(k, False, 1 if k > 32 else 4, 16)
+            a = idx.knn(q, k, form=gts.FORM_FAST, return_ids=True)
+            _pin(idx, k)
+            b = idx.knn(q, k, form=gts.FORM_FAST, return_ids=True)
+            st = idx.search_stats()
+            assert st["blocks"] > 20 * 148, st
+            for x, y in zip(a, b):
+                np.testing.assert_array_equal(x, y, err_msg=f"k={k}")
