@@ -2058,12 +2058,16 @@ static int rerun_failed(gts_index *idx, FastCall &fc, const FastCfg &cfg, int st
     int rc;
     if (stage < 2) {
         int n2 = 0, *r2 = nullptr;
-        if ((rc = fast_run(idx, fc.region, fc.region_bytes, b.sub_q, n, k, cfg, false,
+        // lists that overflowed (or pairs a block-stationary run could not
+        // store) go through the tile filter, whose running bound tightens
+        FastCfg c = cfg;
+        if (stage == 1) c.blk = false;
+        if ((rc = fast_run(idx, fc.region, fc.region_bytes, b.sub_q, n, k, c, false,
                            stage == 1 && r2_prev ? b.sub_r2 : nullptr, b.sub_kth, sub_ids, sub_dis,
                            fc.book[stage + 1].fail, &n2, &r2, st)))
             return rc;
         if (n2 > 0 &&
-            (rc = rerun_failed(idx, fc, cfg, stage + 1, b.sub_q, n2, r2, k, b.sub_kth, sub_ids, sub_dis, st)))
+            (rc = rerun_failed(idx, fc, c, stage + 1, b.sub_q, n2, r2, k, b.sub_kth, sub_ids, sub_dis, st)))
             return rc;
     } else {
         k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 4, (unsigned long long)n);

@@ -51,6 +51,7 @@ constexpr int kBSMax = 6;         // record stages at most
 constexpr int kBAcc = 32;         // TMEM columns per accumulator (kBQ)
 constexpr int kBRing = 16;        // item descriptor slots
 constexpr int kBPre = 8;          // descriptors in flight ahead of the one in use
+constexpr int kBEG = 4;           // epilogue warpgroups
 
 // One column of an item: the query's bound terms against the item's block.
 // x = w - A |d| - 2 v is lb - T for an object (v its MMA product):
@@ -317,8 +318,8 @@ __global__ void __launch_bounds__(256) k_bq_build(const int4 *__restrict__ items
 //             and column), arrive on efree[s].
 // The header of item j stays in its own slot until the epilogue of item
 // j + S - 1 starts (2S slots), so the stage can be refilled early.
-template <bool RANGE>
-__global__ void __launch_bounds__(192, 1) k_fast_blk(FastBlkArgs a)
+template <int EG, bool RANGE>
+__global__ void __launch_bounds__(128 * EG + 64, 1) k_fast_blk(FastBlkArgs a)
 {
     extern __shared__ __align__(1024) unsigned char bsm[];
     unsigned char *base = bsm + ((1024u - (smem_u32(bsm) & 1023u)) & 1023u);
@@ -358,7 +359,8 @@ __global__ void __launch_bounds__(192, 1) k_fast_blk(FastBlkArgs a)
     const uint32_t tmem = ctl.tmem;
     unsigned long long appended = 0;
 
-    if (warp == 4) {
+    constexpr int PW = 4 * EG;   // producer warp; the gather warp follows it
+    if (warp == PW) {
         if (lane == 0) {
             // producer bookkeeping for the bounded drain on error: last item
             // whose copies were issued / waited, last whose MMAs were committed
@@ -440,7 +442,7 @@ __global__ void __launch_bounds__(192, 1) k_fast_blk(FastBlkArgs a)
             }
         }
         __syncwarp();
-    } else if (warp == 5) {
+    } else if (warp == PW + 1) {
         // gather: lane l copies one 16-byte unit (part p, K chunk c, unit u)
         // of every query row of the item
         const int nk = fs.nk, units = 2 * nk * 8;
@@ -498,11 +500,14 @@ __global__ void __launch_bounds__(192, 1) k_fast_blk(FastBlkArgs a)
             if (lane == 0) mbar_arrive(&ctl.gfull[(n_local - 1) % S]);
         }
         __syncwarp();
-    } else if (warp < 4) {
-        const int m = warp * 32 + lane;   // block object, TMEM lane
-        const uint32_t trow = (uint32_t)(warp * 32) << 16;
+    } else {
+        // epilogue warpgroup g takes items g, g + EG, ...; warp w of a group
+        // owns TMEM lanes and block objects 32 (w % 4) .. + 31
+        const int g = warp >> 2, wq = warp & 3;
+        const int m = wq * 32 + lane;   // block object, TMEM lane
+        const uint32_t trow = (uint32_t)(wq * 32) << 16;
         const unsigned lt = (1u << lane) - 1u;
-        for (int j = 0; j < n_local; j++) {
+        for (int j = g; j < n_local; j += EG) {
             const int s = j % S;
             const uint32_t ph = (uint32_t)((j / S) & 1);
             // one verdict per warp: the TMEM loads below are warp-collective
@@ -631,12 +636,16 @@ int fast_blk_enqueue(const FastBlkRun &r, cudaStream_t st, long long *launches)
     const size_t smem = fast_blk_smem(fs, a.nst);
     const unsigned rec_flags = r.capturing ? cudaEventRecordExternal : 0;
     if (r.timed_begin) GTS_CUDA_TRY(cudaEventRecordWithFlags(r.timed_begin, st, rec_flags));
+    // kBEG epilogue warpgroups take turns on the items, so that many items'
+    // list reservations (global atomics) are in flight per SM
     if (r.range) {
-        GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_blk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_fast_blk<true><<<r.nsm, 192, smem, st>>>(a);
+        GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_blk<kBEG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+        k_fast_blk<kBEG, true><<<r.nsm, 128 * kBEG + 64, smem, st>>>(a);
     } else {
-        GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_blk<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_fast_blk<false><<<r.nsm, 192, smem, st>>>(a);
+        GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_blk<kBEG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+        k_fast_blk<kBEG, false><<<r.nsm, 128 * kBEG + 64, smem, st>>>(a);
     }
     if (r.timed_end) GTS_CUDA_TRY(cudaEventRecordWithFlags(r.timed_end, st, rec_flags));
     if (launches) *launches += 4;
