@@ -52,6 +52,7 @@ constexpr int kBAcc = 32;         // TMEM columns per accumulator (kBQ)
 constexpr int kBRing = 16;        // item descriptor slots
 constexpr int kBPre = 8;          // descriptors in flight ahead of the one in use
 constexpr int kBEG = 4;           // epilogue warpgroups
+constexpr int kGRing = 8;         // query-slot ring of the gather warp (items)
 
 // One column of an item: the query's bound terms against the item's block.
 // x = w - A |d| - 2 v is lb - T for an object (v its MMA product):
@@ -85,6 +86,10 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src)
 // this thread's completed generic-proxy shared-memory writes, visible to the
 // async proxy (the tensor core's operand reads)
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void cp_async4(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
@@ -330,7 +335,9 @@ __global__ void __launch_bounds__(128 * EG + 64, 1) k_fast_blk(FastBlkArgs a)
     const uint32_t stage_bytes = rec_pad + 2u * part_bytes;
     BlkCol *heads = reinterpret_cast<BlkCol *>(base + (size_t)S * stage_bytes);   // [2S][kBQ]
     BlkCtl &ctl = *reinterpret_cast<BlkCtl *>(heads + (size_t)2 * S * kBQ);
-    int4 *ring = reinterpret_cast<int4 *>(&ctl + 1);
+    int4 *ring = reinterpret_cast<int4 *>(&ctl + 1);     // producer's item descriptors
+    int4 *gring = ring + kBRing;                          // gather warp's item descriptors
+    int (*sring)[kBQ] = reinterpret_cast<int (*)[kBQ]>(gring + kBRing);   // gather warp's query slots
 
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int G = gridDim.x;
@@ -444,18 +451,32 @@ __global__ void __launch_bounds__(128 * EG + 64, 1) k_fast_blk(FastBlkArgs a)
         __syncwarp();
     } else if (warp == PW + 1) {
         // gather: lane l copies one 16-byte unit (part p, K chunk c, unit u)
-        // of every query row of the item
+        // of every query row of the item.  Nothing on its path waits for a
+        // global load: item descriptors come kBPre items ahead and the
+        // items' query slots kGSlot items ahead, both by cp.async into rings
+        // (copy group j of this warp: item j's rows, descriptor j + kBPre,
+        // slots j + kGSlot).
+        constexpr int kGSlot = 4;
         const int nk = fs.nk, units = 2 * nk * 8;
         const int p = lane / (nk * 8), c = (lane / 8) % nk, u = lane & 7;
         const bool act = lane < units;
         const size_t src_off = (size_t)p * fs.atile_bytes + (size_t)c * (kFT * 128);
         const uint32_t dst_off = rec_pad + (uint32_t)p * part_bytes + (uint32_t)c * (kBQ * 128u);
-        int4 d = make_int4(0, 0, 0, 0);
-        int slot = 0;
-        if (n_local > 0) {
-            d = a.items[blockIdx.x];
-            slot = lane < d.z ? a.bq[d.y + lane] : 0;
-        }
+        auto desc_of = [&](int j) { return a.items + (size_t)blockIdx.x + (size_t)j * G; };
+        auto fetch_slots = [&](int j) {   // query slots of item j (its descriptor is in gring)
+            const int4 d = gring[j % kBRing];
+            if (lane < d.z) cp_async4(&sring[j % kGRing][lane], a.bq + d.y + lane);
+        };
+        // prologue, synchronous: descriptors 0 .. kBPre - 1, slots 0 .. kGSlot - 1
+        if (lane == 0)
+            for (int j = 0; j < kBPre && j < n_local; j++) cp_async16(gring + j % kBRing, desc_of(j));
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncwarp();
+        for (int j = 0; j < kGSlot && j < n_local; j++) fetch_slots(j);
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncwarp();
         bool ok = true;
         for (int j = 0; j < n_local; j++) {
             const int s = j % S;
@@ -469,8 +490,11 @@ __global__ void __launch_bounds__(128 * EG + 64, 1) k_fast_blk(FastBlkArgs a)
                 ok = false;
                 break;
             }
+            // descriptor j and slots j landed: copy groups up to j - 2 are done
+            const int nq = gring[j % kBRing].z;
+            const int slot = lane < nq ? sring[j % kGRing][lane] : 0;
             unsigned char *dst = base + (size_t)s * stage_bytes + dst_off;
-            for (int n = 0; n < d.z; n++) {
+            for (int n = 0; n < nq; n++) {
                 const int sl = __shfl_sync(0xffffffffu, slot, n);
                 if (act) {
                     const int tile = sl >> 7, L = sl & 127;
@@ -478,19 +502,14 @@ __global__ void __launch_bounds__(128 * EG + 64, 1) k_fast_blk(FastBlkArgs a)
                                a.arec + (size_t)tile * fs.arec_bytes + src_off + (size_t)L * 128 + ((u ^ (L & 7)) << 4));
                 }
             }
+            if (lane == 0 && j + kBPre < n_local) cp_async16(gring + (j + kBPre) % kBRing, desc_of(j + kBPre));
+            if (j + kGSlot < n_local) fetch_slots(j + kGSlot);
             cp_async_commit();
-            // the next item's descriptor (its latency overlaps the wait below)
-            int4 dn = d;
-            if (j + 1 < n_local) dn = a.items[(size_t)blockIdx.x + (size_t)(j + 1) * G];
-            if (j >= 1) {   // item j - 1's rows landed: hand them to the producer
+            if (j >= 1) {   // group j - 1 done: item j - 1's rows landed, hand them to the producer
                 cp_async_wait<1>();
                 fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&ctl.gfull[(j - 1) % S]);
-            }
-            if (j + 1 < n_local) {
-                slot = lane < dn.z ? a.bq[dn.y + lane] : 0;
-                d = dn;
             }
         }
         cp_async_wait_all();
@@ -595,7 +614,8 @@ size_t fast_blk_smem(const FastShape &fs, int nst)
 {
     const size_t rec_pad = (fs.rec_bytes + 1023u) & ~1023u;
     const size_t stage = rec_pad + 2 * (size_t)fs.nk * kBQ * 128;
-    return 1024 + (size_t)nst * stage + (size_t)2 * nst * kBHead + sizeof(BlkCtl) + kBRing * sizeof(int4);
+    return 1024 + (size_t)nst * stage + (size_t)2 * nst * kBHead + sizeof(BlkCtl) + 2 * kBRing * sizeof(int4) +
+           (size_t)kGRing * kBQ * sizeof(int);
 }
 
 int fast_blk_stages(const FastShape &fs)
