@@ -1889,6 +1889,7 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
         FastBlkRun br;
         br.args.recs = idx->fast_recs;
         br.args.fs = fs;
+        br.args.k = k;
         br.args.cand_pos = r.cpos;
         br.args.cand_lb = r.clb;
         br.args.cand_ub = r.cub_;
@@ -2569,6 +2570,7 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
             FastBlkRun br;
             br.args.recs = idx->fast_recs;
             br.args.fs = fs;
+            br.args.k = 1;
             br.args.cand_pos = rb.cpos;
             br.args.cand_lb = rb.clb;
             br.args.cand_ub = rb.cub_;

@@ -51,7 +51,7 @@ constexpr int kBSMax = 6;         // record stages at most
 constexpr int kBAcc = 32;         // TMEM columns per accumulator (kBQ)
 constexpr int kBRing = 16;        // item descriptor slots
 constexpr int kBPre = 8;          // descriptors in flight ahead of the one in use
-constexpr int kBEG = 4;           // epilogue warpgroups
+constexpr int kBEG = 3;           // epilogue warpgroups (at most the stages: the phase waits rely on it)
 constexpr int kGRing = 8;         // query-slot ring of the gather warp (items)
 
 // One column of an item: the query's bound terms against the item's block.
@@ -526,23 +526,35 @@ __global__ void __launch_bounds__(128 * EG + 64, 1) k_fast_blk(FastBlkArgs a)
         const int m = wq * 32 + lane;   // block object, TMEM lane
         const uint32_t trow = (uint32_t)(wq * 32) << 16;
         const unsigned lt = (1u << lane) - 1u;
+        const int k = a.k;
         for (int j = g; j < n_local; j += EG) {
             const int s = j % S;
             const uint32_t ph = (uint32_t)((j / S) & 1);
+            // the copies of item j landed (record tail, header): visible here
+            mbar_wait(&ctl.full[s], ph, kFWait);
+            const BlkCol *cols = heads + (size_t)(j % (2 * S)) * kBQ;
+            // column lane (kBQ = 32 columns): the query's bound now -- other
+            // items may have lowered it since the header was built -- as
+            // r2c and as rtc = min(RT, r2c - T), read while the MMA runs
+            float r2c = 0.f, rtc = 0.f;
+            {
+                const BlkCol cl = cols[lane];
+                if (cl.qi >= 0) {
+                    r2c = RANGE ? cl.RT + cl.T : __int_as_float(*(volatile const int *)(a.r2_bits + cl.qi));
+                    rtc = RANGE ? cl.RT : fminf(cl.RT, r2c - cl.T);
+                }
+            }
             // one verdict per warp: the TMEM loads below are warp-collective
             if (!__all_sync(0xffffffffu, mbar_wait(&ctl.mmad[s], ph, kFWait))) {
                 atomicMax(&ctl.err, 4);
                 break;
             }
             tc_fence_after();
-            // the copies of item j landed (record tail, header): visible here
-            mbar_wait(&ctl.full[s], ph, kFWait);
             const float *tail = reinterpret_cast<const float *>(base + (size_t)s * stage_bytes + fs.btile_bytes);
             const float w = tail[kTailW + m], dn = tail[kTailDn + m];
             const int blk = ctl.blk[s], nq = ctl.ncol[s];
             __syncwarp();
             if (lane == 0) mbar_arrive(&ctl.rfree[s]);
-            const BlkCol *cols = heads + (size_t)(j % (2 * S)) * kBQ;
             const int slot = blk * kFB + m;
             for (int c0 = 0; c0 < nq; c0 += 16) {
                 uint32_t v[16];
@@ -553,9 +565,10 @@ __global__ void __launch_bounds__(128 * EG + 64, 1) k_fast_blk(FastBlkArgs a)
 #pragma unroll
                 for (int u = 0; u < 16; u++) {
                     const BlkCol cc = cols[c0 + u];
+                    const float rt = __shfl_sync(0xffffffffu, rtc, c0 + u);
                     const float x = fmaf(-2.f, __uint_as_float(v[u]), fmaf(-cc.A, dn, w));
                     const bool ok = cc.qi >= 0 && c0 + u < nq;
-                    pass |= (ok && x <= cc.RT ? 1u : 0u) << u;
+                    pass |= (ok && x <= rt ? 1u : 0u) << u;
                     if constexpr (RANGE) inside |= (ok && x + 2.f * fmaf(cc.A, dn, cc.eb) < cc.RLT ? 1u : 0u) << u;
                 }
                 if constexpr (RANGE) {
@@ -584,16 +597,44 @@ __global__ void __launch_bounds__(128 * EG + 64, 1) k_fast_blk(FastBlkArgs a)
 #pragma unroll
                 for (int u = 0; u < 16; u++) {
                     const int b = __shfl_sync(0xffffffffu, mybase, u);
-                    if (!((pass >> u) & 1u)) continue;
-                    const int at = b + __popc(bal[u] & lt);
-                    if (at >= kFCand) continue;
-                    const BlkCol cc = cols[c0 + u];
-                    const float lb = cc.T + fmaf(-2.f, __uint_as_float(v[u]), fmaf(-cc.A, dn, w));
-                    const float ub = lb + 2.f * fmaf(cc.A, dn, cc.eb);
-                    const size_t o = (size_t)cc.qi * kFCand + at;
-                    a.cand_pos[o] = slot;
-                    a.cand_lb[o] = lb;
-                    a.cand_ub[o] = ub;
+                    float ub = INFINITY;
+                    if ((pass >> u) & 1u) {
+                        const BlkCol cc = cols[c0 + u];
+                        const float lb = cc.T + fmaf(-2.f, __uint_as_float(v[u]), fmaf(-cc.A, dn, w));
+                        ub = lb + 2.f * fmaf(cc.A, dn, cc.eb);
+                        const int at = b + __popc(bal[u] & lt);
+                        if (at < kFCand) {
+                            const size_t o = (size_t)cc.qi * kFCand + at;
+                            a.cand_pos[o] = slot;
+                            a.cand_lb[o] = lb;
+                            a.cand_ub[o] = ub;
+                        }
+                    }
+                    if constexpr (!RANGE) {
+                        // k distinct objects of this warp with upper bounds
+                        // below the query's bound: their k-th smallest upper
+                        // bound is a bound on its k-th distance (the tile
+                        // filter's running bound, per warp and block)
+                        const float r2u = __shfl_sync(0xffffffffu, r2c, c0 + u);
+                        const unsigned below = __ballot_sync(0xffffffffu, ub < r2u);
+                        if (k <= 32 && __popc(below) >= k) {
+                            float x = ub < r2u ? ub : INFINITY, mn = x;
+                            for (int it = 0; it < k; it++) {
+                                mn = x;
+#pragma unroll
+                                for (int o = 16; o > 0; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+                                if (it == k - 1) break;
+                                const unsigned own = __ballot_sync(0xffffffffu, x == mn);
+                                if (lane == __ffs(own) - 1) x = INFINITY;
+                            }
+                            const BlkCol cc = cols[c0 + u];
+                            if (lane == 0) atomicMin(a.r2_bits + cc.qi, __float_as_int(fmaxf(mn, 0.f)));
+                            if (lane == c0 + u) {
+                                r2c = fminf(r2c, mn);
+                                rtc = fminf(rtc, mn - cc.T);
+                            }
+                        }
+                    }
                 }
             }
             tc_fence_before();

@@ -19,6 +19,7 @@ struct FastBlkArgs {
     const int *bq;               // query slots of the pairs
     const unsigned char *arec;   // tile records: the queries' operand rows
     FastShape fs;
+    int k;                       // kNN: neighbours per query (the running bound); range: unused
     int nst;                     // record stages
     int *cand_pos;               // [qnum][kFCand]
     float *cand_lb, *cand_ub;
