@@ -665,7 +665,8 @@ int fast_blk_stages(const FastShape &fs)
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    for (int s = kBSMax; s >= 2; s--)
+    // at least one stage per epilogue warpgroup
+    for (int s = kBSMax; s >= std::max(2, kBEG); s--)
         if (fast_blk_smem(fs, s) <= (size_t)optin) return s;
     return 0;
 }
