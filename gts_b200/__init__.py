@@ -302,7 +302,7 @@ class Index:
 
     def fast_range_variant(self, variant=None) -> int:
         """Filter of the fast range counts: 0 the block-stationary one where
-        it fits (default), 1 the tile one; None leaves it.  Returns it."""
+        it fits, 1 the tile one (default); None leaves it.  Returns it."""
         cur = C.c_int()
         _check(self._lib.gts_fast_range_variant(self._h, -1 if variant is None else int(variant), C.byref(cur)))
         return cur.value

@@ -1468,11 +1468,13 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
     }   // for wi
 }
 
+// Sort keys of the queries: the block of their slot (tiles group queries
+// by block order; the order inside a block does not matter).
 __global__ void k_fast_keys(const int *qids, int qnum, const int *pos_of, int *keys, int *vals)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < qnum) {
-        keys[i] = pos_of[qids[i]];
+        keys[i] = pos_of[qids[i]] / kFB;
         vals[i] = i;
     }
 }
@@ -1821,9 +1823,9 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     idx->kernel_launches++;
     k_fast_keys<<<(qnum + 255) / 256, 256, 0, st>>>(d_qids, qnum, bs.pos, r.keys, r.vals);
     idx->kernel_launches++;
-    // slots are below nb * 128: sort only the bits they use
+    // block ids are below nb: sort only the bits they use
     int key_bits = 1;
-    while (key_bits < 32 && (1ll << key_bits) < (long long)nb * kFB) key_bits++;
+    while (key_bits < 32 && (1ll << key_bits) < (long long)nb) key_bits++;
     size_t cb = r.cub_bytes;
     GTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(r.cub, cb, r.keys, r.skeys, r.vals, r.order, qnum, 0, key_bits,
                                                  st));
@@ -2510,7 +2512,7 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
     GTS_CUDA_TRY(cudaMemsetAsync(idx->d_status, 0, sizeof(int), st));
     if (!idx->keep_stats) GTS_CUDA_TRY(cudaMemsetAsync(idx->d_stats, 0, kStatsN * sizeof(unsigned long long), st));
     int key_bits = 1;
-    while (key_bits < 32 && (1ll << key_bits) < (long long)nb * kFB) key_bits++;
+    while (key_bits < 32 && (1ll << key_bits) < (long long)nb) key_bits++;
     for (int q0 = 0; q0 < qnum; q0 += qc) {
         const int n = std::min(qc, qnum - q0);
         const int *dq = d_qids + q0;

@@ -42,7 +42,7 @@ struct gts_index {
     // autotuned fast-form configuration per k (fast.cu): 0 = not tuned, else
     // 1 | learned << 1 | column groups << 2 | blocks per item << 8
     int fast_cfg[65] = {};
-    int range_variant = 0;   // fast range counts: 0 the block-stationary filter where it fits, 1 the tile filter
+    int range_variant = 1;   // fast range counts: 0 the block-stationary filter where it fits, 1 the tile filter
     // autotuned threads per query CTA of the plain traversal per search mode
     // (kNN, range count, range ids; search.cu), 0 = not tuned
     int plain_nt[3] = {};

@@ -172,7 +172,7 @@ int gts_fast_config(const gts_index *idx, int k, int *tuned, int *learned, int *
 int gts_fast_config_set(gts_index *idx, int k, int learned, int col_groups, int item_blocks, int variant);
 
 /* The filter of GTS_FORM_FAST range counts: variant 0 the block-stationary
- * filter where it fits (dim <= 128; the default), 1 the tile filter; -1
+ * filter where it fits (dim <= 128), 1 the tile filter (the default); -1
  * leaves it.  *current (nullable) receives the setting. */
 int gts_fast_range_variant(gts_index *idx, int variant, int *current);
 
