@@ -1936,15 +1936,21 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 1ull);
     idx->kernel_launches++;
     // light recheck over every query, then the full one over those with more
-    // than 128 candidates (a persistent grid of a few CTAs per SM walking
-    // their list)
-    const int final_grid = 4 * nsm;
+    // than 128 candidates: a persistent grid, as many CTAs as fit on the SMs,
+    // walking their list
+    auto full_grid = [&](const void *fn) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, 0) != cudaSuccess || per_sm < 1)
+            per_sm = 4;
+        return std::min(qnum, per_sm * nsm);
+    };
     if (fs.kp <= kFResKp) {
         k_fast_final<kFResKp, kFinB, 128><<<qnum, 128, 0, st>>>(
             idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
             r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, r.heavy, r.ctr + 4, nullptr, nullptr,
             idx->d_stats);
-        k_fast_final<kFResKp, kFinB, kFCand><<<std::min(qnum, final_grid), 128, 0, st>>>(
+        k_fast_final<kFResKp, kFinB, kFCand><<<full_grid((const void *)k_fast_final<kFResKp, kFinB, kFCand>), 128, 0,
+                                                st>>>(
             idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
             r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, nullptr, nullptr, r.heavy, r.ctr + 4,
             idx->d_stats);
@@ -1953,7 +1959,8 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
             idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
             r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, r.heavy, r.ctr + 4, nullptr, nullptr,
             idx->d_stats);
-        k_fast_final<kFMaxKp, kFinB / 2, kFCand><<<std::min(qnum, final_grid), 128, 0, st>>>(
+        k_fast_final<kFMaxKp, kFinB / 2, kFCand><<<full_grid((const void *)k_fast_final<kFMaxKp, kFinB / 2, kFCand>),
+                                                    128, 0, st>>>(
             idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
             r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, nullptr, nullptr, r.heavy, r.ctr + 4,
             idx->d_stats);
@@ -2087,13 +2094,16 @@ static int rerun_failed(gts_index *idx, FastCall &fc, const FastCfg &cfg, int st
     return GTS_OK;
 }
 
+// Captures of one batch shape (with different argument buffers) kept at most.
+constexpr int kGraphShapeMax = 4;
+
 // One batch (at most one filter run) through the CUDA graph of the filter
 // pass: the pass (sort, seeds, pruning, filter, recheck: 11-12 kernels and
 // the CUB sort) is captured once per batch shape and argument buffers and
 // replayed on the handle's own stream.  The host then reads the failure
 // count and runs any re-answer stage directly.  Returns 1 (nothing done)
-// when the caller's buffers moved since the last capture as well: such
-// callers are better served by direct launches.  The caller has reset
+// when this shape was captured kGraphShapeMax times with other buffers
+// already: such callers are better served by direct launches.  The caller has reset
 // status and counters on st.
 static int fast_search_graph(gts_index *idx, FastCall &fc, const FastCfg &cfg, const int *d_qids, int qnum, int k,
                              float *d_kth, int *d_ids, float *d_dists, cudaStream_t st)
@@ -2114,24 +2124,22 @@ static int fast_search_graph(gts_index *idx, FastCall &fc, const FastCfg &cfg, c
                               (long long)(uintptr_t)d_qids, (long long)(uintptr_t)d_kth,
                               (long long)(uintptr_t)d_ids ^ ((long long)(uintptr_t)d_dists << 1)};
     constexpr int NS = gts_index::kGraphSlots;
-    int slot = -1, shape_slot = -1;
+    int slot = -1, same_shape = 0;
     for (int s = 0; s < NS; s++) {
         if (!idx->graph_exec[s]) continue;
         bool same = true, shape = true;
         for (int i = 0; i < 8; i++) same = same && idx->graph_key[s][i] == key[i];
         for (int i = 0; i < 5; i++) shape = shape && idx->graph_key[s][i] == key[i];
         if (same) slot = s;
-        else if (shape) shape_slot = s;
+        else if (shape) same_shape++;
     }
     if (slot < 0) {
-        // the same shape with other buffers twice in a row: launch directly
-        if (shape_slot >= 0 && idx->graph_moved) return 1;
-        idx->graph_moved = shape_slot >= 0;
-        // capture into the slot of that shape, else a free or the least recently used one
-        slot = shape_slot;
-        if (slot < 0)
-            for (int s = 0; s < NS; s++)
-                if (!idx->graph_exec[s]) { slot = s; break; }
+        // a caller whose buffers keep moving (four captures of this shape
+        // with other buffers already) is better served by direct launches
+        if (same_shape >= kGraphShapeMax) return 1;
+        // capture into a free slot, else the least recently used one
+        for (int s = 0; s < NS && slot < 0; s++)
+            if (!idx->graph_exec[s]) slot = s;
         if (slot < 0) {
             slot = 0;
             for (int s = 1; s < NS; s++)
@@ -2164,8 +2172,6 @@ static int fast_search_graph(gts_index *idx, FastCall &fc, const FastCfg &cfg, c
         }
         for (int i = 0; i < 8; i++) idx->graph_key[slot][i] = key[i];
         idx->graph_kernels[slot] = in_graph;
-    } else {
-        idx->graph_moved = false;
     }
     idx->graph_used[slot] = ++idx->graph_clock;
     GTS_CUDA_TRY(cudaEventRecord(idx->graph_ev[0], st));

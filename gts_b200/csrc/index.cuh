@@ -67,7 +67,7 @@ struct gts_index {
     // up to kGraphSlots captured filter passes, one per batch shape and
     // argument buffers (batches of a few shapes in turn, such as one per k,
     // each replay their own), least recently used replaced
-    static constexpr int kGraphSlots = 4;
+    static constexpr int kGraphSlots = 16;
     cudaGraphExec_t graph_exec[kGraphSlots] = {};
     long long graph_key[kGraphSlots][8] = {};
     long long graph_used[kGraphSlots] = {};
@@ -76,7 +76,6 @@ struct gts_index {
     bool use_graphs = true;
     long long graph_launches = 0;
     long long graph_clock = 0;
-    bool graph_moved = false;      // the last capture was for an existing shape with moved argument buffers
     // second stream of the filter pass: the own-block seeds run on it while
     // the query sort and tile operands run on the first (fast.cu)
     cudaStream_t side_stream = nullptr;

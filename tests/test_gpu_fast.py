@@ -219,3 +219,25 @@ def test_graphs_of_alternating_batch_shapes(oracle):
             for (q, k), w in zip(batches, want):
                 np.testing.assert_array_equal(idx.knn(q, k, form=gts.FORM_FAST), w, err_msg=f"k={k}")
         assert idx.fast_graphs() - n0 == 9
+
+
+def test_graphs_of_one_shape_with_moving_buffers(oracle):
+    """Device-buffer calls of one batch shape with new output buffers each
+    time: the first four buffer sets are captured and replayed, further ones
+    launch directly; every answer is the same."""
+    import torch
+    rows = G.gmm_rows(20000, 64, 16, 0.25, seed=131)
+    ds = oracle.Dataset(2, rows)
+    q = G.query_ids(20000, 300, seed=132)
+    want = oracle.knn_brute(ds, q, 8)[0]
+    with gts.Index(rows, 2, max_h=5) as idx:
+        d_q = torch.from_numpy(q).cuda()
+        outs = [torch.empty(len(q), dtype=torch.float32, device="cuda") for _ in range(6)]
+        n0 = idx.fast_graphs()
+        for rep in range(2):
+            for out in outs:
+                idx.knn_device(d_q.data_ptr(), len(q), 8, out.data_ptr(), form=gts.FORM_FAST)
+                torch.cuda.synchronize()
+                np.testing.assert_array_equal(out.cpu().numpy(), want)
+        # four captures replayed twice each; the other two buffer sets direct
+        assert idx.fast_graphs() - n0 == 8
