@@ -285,6 +285,14 @@ class Index:
         return {"tuned": bool(v[0].value), "learned_seed": bool(v[1].value), "col_groups": v[2].value,
                 "item_blocks": v[3].value, "streamed": v[4].value == 1, "by_block": v[4].value == 2}
 
+    def fast_seeds(self, qids, k: int) -> np.ndarray:
+        """The fast form's starting bound on each query's squared k-th
+        distance (made with the filter records; see gts_fast_seeds)."""
+        q = np.ascontiguousarray(qids, dtype=np.int32)
+        out = np.empty(len(q), np.float32)
+        _check(self._lib.gts_fast_seeds(self._h, _ip(q), len(q), k, _fp(out)))
+        return out
+
     def fast_graphs(self, on=None) -> int:
         """Turn the captured filter graph on/off (None: leave it); returns the
         number of graph replays so far."""

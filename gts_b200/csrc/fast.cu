@@ -270,82 +270,204 @@ __global__ void __launch_bounds__(128) k_fast_arec(const float *__restrict__ row
     info[lq] = make_int4(qi, __float_as_int((float)acc), __float_as_int((float)sqrt(acc)), 0);
 }
 
-// One CTA per query: the k-th smallest FP32 squared distance inside the
-// query's own block (the query is one of its objects), widened past every
-// rounding difference to the reference's value, lowers the query's bound.
-// The block's rows are read from the slot-ordered copy (one contiguous
-// 128 x kp range): one warp per 32 rows, lane l holding the float4 columns
-// l, l + 32 and l + 64 (dimensions 4l.., 128 + 4l.., 256 + 4l.. up to kp),
-// sixteen rows in flight per warp; warp 0 then takes out the smallest value
-// k - 1 times (four values per lane).
-__global__ void __launch_bounds__(128) k_fast_seed(const float *__restrict__ rows, const int *__restrict__ qids,
-                                                   FastSummary bs, int dim, int kp, int k, int *__restrict__ r2_bits)
+// Seeds made once with the records.  Queries are objects, so a bound on a
+// query's k-th distance can be computed per object ahead of any call: the
+// k-th smallest distance from the object to the objects of its own block
+// and of the kSeedNbr blocks whose centres lie nearest to its block's (the
+// object itself counts, at distance 0).  Any k of those objects bound the
+// query's k-th distance, and eight blocks hold far more close neighbours
+// than one, so the seed sits much nearer the answer than the own-block
+// k-th distance: fewer blocks survive the pruning and fewer candidates the
+// filter.  Stored for k = 1, 2, 4, .., 64 (a call with another k reads the
+// next power of two: a bound for the larger k bounds every smaller k).
+
+// The kSeedNbr blocks with the nearest centres (FP32, ties by block id),
+// -1 where there are fewer blocks.  One warp per block b, eight per CTA;
+// the CTA stages 32 centres at a time in shared memory and lane l measures
+// centre l of the stage against its warp's centre.
+constexpr int kNbrWarps = 8;
+__global__ void __launch_bounds__(32 * kNbrWarps) k_fast_nbrs(FastSummary bs, int nb, int kp,
+                                                              int *__restrict__ nbr)
 {
-    __shared__ float v[kFB];
-    const int q = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    const int qid = qids[q];
-    const int base = bs.pos[qid] / kFB * kFB;
-    const bool valid = bs.ids[base + t] >= 0;   // valid slots come first
-    const int cnt = __syncthreads_count(valid);
-    if (cnt < k) return;
-    const unsigned vm = __ballot_sync(0xffffffffu, valid);   // this warp's 32 rows
-    const float *qr = rows + (size_t)qid * dim;
-    constexpr int kSeedCols = kFMaxKp / 128 + 1;   // float4 columns per lane (kp <= 320)
-    float qv[kSeedCols][4];
-    bool act[kSeedCols];
+    extern __shared__ float nsm[];   // [kNbrWarps][kp] own centres, then [32][kp + 4] staged centres
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int ks = kp + 4;
+    float *own = nsm + warp * kp;
+    float *stg = nsm + kNbrWarps * kp;
+    const int b = blockIdx.x * kNbrWarps + warp;
+    for (int d = lane; d < kp; d += 32) own[d] = b < nb ? bs.cen[(size_t)b * kp + d] : 0.f;
+    float bd[kSeedNbr];
+    int bi[kSeedNbr];
 #pragma unroll
-    for (int c = 0; c < kSeedCols; c++) {
-        const int j0 = 4 * (lane + 32 * c);
-        act[c] = j0 < kp;
-#pragma unroll
-        for (int e = 0; e < 4; e++) qv[c][e] = (act[c] && j0 + e < dim) ? qr[j0 + e] : 0.f;
+    for (int i = 0; i < kSeedNbr; i++) {
+        bd[i] = FLT_MAX;
+        bi[i] = -1;
     }
-    const float *pb = bs.prow + (size_t)(base + warp * 32) * kp + 4 * lane;
+    for (int j0 = 0; j0 < nb; j0 += 32) {
+        __syncthreads();
+        for (int e = t; e < 32 * kp; e += blockDim.x) {
+            const int r = e / kp, d = e - r * kp;
+            stg[r * ks + d] = j0 + r < nb ? bs.cen[(size_t)(j0 + r) * kp + d] : 0.f;
+        }
+        __syncthreads();
+        const int j = j0 + lane;
+        if (b >= nb || j >= nb || j == b) continue;
+        float acc = 0.f;
+        for (int d = 0; d < kp; d += 4) {
+            const float4 c4 = *reinterpret_cast<const float4 *>(stg + lane * ks + d);
+            const float4 o4 = *reinterpret_cast<const float4 *>(own + d);
+            const float e0 = c4.x - o4.x, e1 = c4.y - o4.y, e2 = c4.z - o4.z, e3 = c4.w - o4.w;
+            acc = fmaf(e3, e3, fmaf(e2, e2, fmaf(e1, e1, fmaf(e0, e0, acc))));
+        }
+        if (acc < bd[kSeedNbr - 1]) {   // sorted insertion (j grows, so ties keep the smaller id)
+            float v = acc;
+            int vi = j;
 #pragma unroll
-    for (int i0 = 0; i0 < 32; i0 += 16) {
-        float acc[16];
-#pragma unroll
-        for (int r = 0; r < 16; r++) {
-            acc[r] = 0.f;
-            const bool rv = (vm >> (i0 + r)) & 1u;
-#pragma unroll
-            for (int c = 0; c < kSeedCols; c++) {
-                float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (act[c] && rv) o = *reinterpret_cast<const float4 *>(pb + (size_t)(i0 + r) * kp + 128 * c);
-                const float e0 = o.x - qv[c][0], e1 = o.y - qv[c][1], e2 = o.z - qv[c][2], e3 = o.w - qv[c][3];
-                acc[r] = fmaf(e3, e3, fmaf(e2, e2, fmaf(e1, e1, fmaf(e0, e0, acc[r]))));
+            for (int i = 0; i < kSeedNbr; i++) {
+                if (v < bd[i]) {
+                    const float tv = bd[i];
+                    const int ti = bi[i];
+                    bd[i] = v;
+                    bi[i] = vi;
+                    v = tv;
+                    vi = ti;
+                }
             }
         }
+    }
+    if (b >= nb) return;
+    // the kSeedNbr smallest of the 32 lanes' lists: each round the lane
+    // holding the smallest head (ties: smaller id) pops it
+    int head = 0;
+    for (int r = 0; r < kSeedNbr; r++) {
+        float v = FLT_MAX;
+        int vi = INT_MAX;
 #pragma unroll
-        for (int r = 0; r < 16; r++) {
-            const float s = warp_sum(acc[r]);
-            if (lane == 0) v[warp * 32 + i0 + r] = ((vm >> (i0 + r)) & 1u) ? s : FLT_MAX;
+        for (int i = 0; i < kSeedNbr; i++)
+            if (i == head) {
+                v = bd[i];
+                vi = bi[i] < 0 ? INT_MAX : bi[i];
+            }
+        float mv = v;
+        int mi = vi;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_xor_sync(0xffffffffu, mv, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, mi, o);
+            if (ov < mv || (ov == mv && oi < mi)) {
+                mv = ov;
+                mi = oi;
+            }
+        }
+        if (vi == mi && vi != INT_MAX) head++;
+        if (lane == 0) nbr[(size_t)b * kSeedNbr + r] = mi == INT_MAX ? -1 : mi;
+    }
+}
+
+// The seed table: one CTA per block b, warp w taking objects w, w + 4, ...
+// For each of the blocks (b, then its neighbours) the block's FP32 rows are
+// staged in shared memory ([128][kp + 4]); lane l sums the squared FP32
+// differences of rows l, l + 32, l + 64, l + 96 against the object's row in
+// dimension order (fused multiply-adds, as the reference's leaf loop runs
+// them), and the object's 64 smallest values so far (in shared memory,
+// ascending) are merged with the new values below the 64th by ranking.
+// A sum of at most 320 non-negative FP32 terms is within 322 * 2^-24 <
+// 2e-5 relative of the exact sum of the same FP32 differences squared, the
+// value the reference's FP64 sum rounds, so widening by (1 + 4e-5) gives a
+// certified bound on the reference's k-th squared distance.  FLT_MAX where
+// the blocks hold fewer than k objects (no seed).
+__global__ void __launch_bounds__(128) k_fast_selfk(FastSummary bs, int kp, const int *__restrict__ nbr)
+{
+    extern __shared__ float ssm[];
+    const int b = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int ks = kp + 4;
+    float *srow = ssm;                                  // [128][ks] the staged block's rows
+    float *best = srow + (size_t)kFB * ks;              // [128][kSeedBest] per object, ascending
+    float *obuf = best + (size_t)kFB * kSeedBest + warp * (kp + 3 * kSeedBest);   // [kp] object row
+    float *sc = obuf + kp;                              // [3 * kSeedBest] merge scratch
+    __shared__ unsigned vmask[kFB / 32], omask[kFB / 32];
+    const unsigned own_valid = __ballot_sync(0xffffffffu, bs.ids[b * kFB + t] >= 0);
+    if (lane == 0) omask[warp] = own_valid;
+    for (int i = t; i < kFB * kSeedBest; i += blockDim.x) best[i] = FLT_MAX;
+    int cnt = 0;   // objects in the blocks used so far
+    for (int s = 0; s <= kSeedNbr; s++) {
+        const int j = s == 0 ? b : nbr[(size_t)b * kSeedNbr + s - 1];
+        if (j < 0) break;
+        __syncthreads();
+        // stage block j's rows and validity
+        const float4 *src = reinterpret_cast<const float4 *>(bs.prow + (size_t)j * kFB * kp);
+        for (int e = t; e < kFB * kp / 4; e += blockDim.x) {
+            const int r = e / (kp / 4), d4 = e - r * (kp / 4);
+            *reinterpret_cast<float4 *>(srow + (size_t)r * ks + 4 * d4) = src[e];
+        }
+        const bool jv = bs.ids[j * kFB + t] >= 0;
+        const unsigned jm = __ballot_sync(0xffffffffu, jv);
+        if (lane == 0) vmask[warp] = jm;   // valid rows of block j
+        cnt += __syncthreads_count(jv);    // also: rows and masks visible
+        for (int m = warp; m < kFB; m += 4) {
+            if (!((omask[m >> 5] >> (m & 31)) & 1u)) continue;
+            const float *orow = bs.prow + ((size_t)b * kFB + m) * kp;
+            for (int d = lane; d < kp; d += 32) obuf[d] = orow[d];
+            __syncwarp();
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            for (int d = 0; d < kp; d += 4) {
+                const float4 q4 = *reinterpret_cast<const float4 *>(obuf + d);
+#pragma unroll
+                for (int h = 0; h < 4; h++) {
+                    const float4 o4 = *reinterpret_cast<const float4 *>(srow + (size_t)(lane + 32 * h) * ks + d);
+                    const float e0 = o4.x - q4.x, e1 = o4.y - q4.y, e2 = o4.z - q4.z, e3 = o4.w - q4.w;
+                    acc[h] = fmaf(e3, e3, fmaf(e2, e2, fmaf(e1, e1, fmaf(e0, e0, acc[h]))));
+                }
+            }
+            float *bm = best + (size_t)m * kSeedBest;
+            const float thr = bm[kSeedBest - 1];
+            // survivors (below the current 64th smallest) after the 64 kept values
+            sc[lane] = bm[lane];
+            sc[lane + 32] = bm[lane + 32];
+            int n = kSeedBest;
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                const bool rv = (vmask[h] >> lane) & 1u;
+                const bool keep = rv && acc[h] < thr;
+                const unsigned km = __ballot_sync(0xffffffffu, keep);
+                if (keep) sc[n + __popc(km & ((1u << lane) - 1u))] = acc[h];
+                n += __popc(km);
+            }
+            __syncwarp();
+            if (n > kSeedBest) {
+                for (int i = lane; i < n; i += 32) {
+                    const float v = sc[i];
+                    int rank = 0;
+                    for (int q = 0; q < n; q++) {
+                        const float y = sc[q];
+                        rank += (y < v || (y == v && q < i)) ? 1 : 0;
+                    }
+                    if (rank < kSeedBest) bm[rank] = v;
+                }
+            }
+            __syncwarp();
         }
     }
     __syncthreads();
-    if (warp != 0) return;
-    float x[4];
-#pragma unroll
-    for (int m = 0; m < 4; m++) x[m] = v[lane + 32 * m];
-    float mn = FLT_MAX;
-    for (int it = 0; it < k; it++) {
-        const float lm = fminf(fminf(x[0], x[1]), fminf(x[2], x[3]));
-        mn = lm;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-        if (it == k - 1) break;
-        const unsigned own = __ballot_sync(0xffffffffu, lm == mn);
-        if (lane == __ffs(own) - 1) {
-            if (x[0] == mn) x[0] = FLT_MAX;
-            else if (x[1] == mn) x[1] = FLT_MAX;
-            else if (x[2] == mn) x[2] = FLT_MAX;
-            else x[3] = FLT_MAX;
+    for (int m = warp; m < kFB; m += 4) {
+        int *out = bs.selfk + ((size_t)b * kFB + m) * kSelfK;
+        const float *bm = best + (size_t)m * kSeedBest;
+        if (lane < kSelfK) {
+            int v = __float_as_int(FLT_MAX);
+            if (lane < kSelfKN && ((omask[m >> 5] >> (m & 31)) & 1u) && cnt >= (1 << lane))
+                v = __float_as_int(bm[(1 << lane) - 1] * (1.f + 4e-5f));
+            out[lane] = v;
         }
     }
-    // FP32 sum of at most 320 non-negative terms (at most 12 per lane, then a
-    // 32-lane tree): relative error < 2^-19 against the reference's FP64 sum
-    // of the same FP32 differences
-    if (lane == 0) atomicMin(&r2_bits[q], __float_as_int(mn * (1.f + 3e-5f)));
+}
+
+// Seeds from the table: one thread per query (jk: the smallest power of two
+// 2^jk >= k).
+__global__ void k_fast_seed_tab(const int *__restrict__ qids, int qnum, const int *__restrict__ pos_of,
+                                const int *__restrict__ selfk, int jk, int *__restrict__ r2_bits)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < qnum) atomicMin(&r2_bits[i], selfk[(size_t)pos_of[qids[i]] * kSelfK + jk]);
 }
 
 // ---------------------------------------------------------------- pruning
@@ -1685,7 +1807,19 @@ static int fast_prepare(gts_index *idx, cudaStream_t st)
     k_fast_prep<<<nb, kFB, 0, st>>>(idx->dim, idx->rows, recs, fs, bs);
     k_fast_prows<<<nb, kFB, 0, st>>>(idx->dim, fs.kp, idx->rows, bs.ids, bs.prow);
     k_fast_sbprep<<<nsb, 256, 0, st>>>(idx->dim, idx->rows, fs, bs);
-    cudaError_t e = cudaGetLastError();
+    // the seed table: neighbour blocks by centre, then per object the k-th
+    // distances over its block and those
+    const size_t nbrs_smem = sizeof(float) * ((size_t)kNbrWarps * fs.kp + 32 * (size_t)(fs.kp + 4));
+    const size_t selfk_smem =
+        sizeof(float) * ((size_t)kFB * (fs.kp + 4) + (size_t)kFB * kSeedBest + 4 * (size_t)(fs.kp + 3 * kSeedBest));
+    cudaError_t e = cudaFuncSetAttribute(k_fast_nbrs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nbrs_smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_fast_selfk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)selfk_smem);
+    if (e == cudaSuccess) {
+        k_fast_nbrs<<<(nb + kNbrWarps - 1) / kNbrWarps, 32 * kNbrWarps, nbrs_smem, st>>>(bs, nb, fs.kp, bs.nbr);
+        k_fast_selfk<<<nb, kFB, selfk_smem, st>>>(bs, fs.kp, bs.nbr);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         cudaFree(recs);
@@ -1819,7 +1953,9 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
         GTS_CUDA_TRY(cudaEventRecord(idx->side_ev[0], st));
         GTS_CUDA_TRY(cudaStreamWaitEvent(ss, idx->side_ev[0], 0));
     }
-    k_fast_seed<<<qnum, 128, 0, ss>>>(idx->rows, d_qids, bs, idx->dim, fs.kp, k, r.r2);
+    int jk = 0;   // the table's k: the smallest power of two >= k (k <= kFMaxK = 2^(kSelfKN - 1))
+    while ((1 << jk) < k) jk++;
+    k_fast_seed_tab<<<(qnum + 255) / 256, 256, 0, ss>>>(d_qids, qnum, bs.pos, bs.selfk, jk, r.r2);
     idx->kernel_launches++;
     k_fast_keys<<<(qnum + 255) / 256, 256, 0, st>>>(d_qids, qnum, bs.pos, r.keys, r.vals);
     idx->kernel_launches++;
@@ -2730,6 +2866,51 @@ extern "C" int gts_fast_graphs(gts_index *idx, int on, long long *replays)
         if (!idx->use_graphs) gts::graph_invalidate(idx);
     }
     if (replays) *replays = idx->graph_launches;
+    return GTS_OK;
+}
+
+namespace gts {
+__global__ void k_fast_seed_get(const int *__restrict__ qids, int qnum, const int *__restrict__ pos_of,
+                                const int *__restrict__ selfk, int jk, int *__restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < qnum) out[i] = selfk[(size_t)pos_of[qids[i]] * kSelfK + jk];
+}
+}  // namespace gts
+
+extern "C" int gts_fast_seeds(gts_index *idx, const int *qids, int qnum, int k, float *seeds_out)
+{
+    if (!idx || qnum < 0 || (qnum > 0 && (!qids || !seeds_out)) || k < 1 || k > gts::kFMaxK) {
+        gts_set_error("gts_fast_seeds: invalid argument (k in [1, %d])", gts::kFMaxK);
+        return GTS_ERR_INVALID;
+    }
+    if (!idx->fast_recs) {
+        gts_set_error("gts_fast_seeds: the index holds no filter records (gts_index_prepare with GTS_FORM_FAST)");
+        return GTS_ERR_INVALID;
+    }
+    for (int i = 0; i < qnum; i++)
+        if (qids[i] < 0 || qids[i] >= idx->num) {
+            gts_set_error("gts_fast_seeds: query id %d out of range", qids[i]);
+            return GTS_ERR_INVALID;
+        }
+    if (qnum == 0) return GTS_OK;
+    const gts::FastShape fs = gts::fast_shape(idx->dim);
+    const gts::FastSummary bs = gts::fast_summary(idx->fast_recs, fs, idx->fast_nb, idx->fast_nsb, idx->num);
+    int jk = 0;
+    while ((1 << jk) < k) jk++;
+    int *d = nullptr;
+    GTS_CUDA_TRY(cudaMalloc(&d, 2 * sizeof(int) * (size_t)qnum));
+    cudaError_t e = cudaMemcpy(d, qids, sizeof(int) * (size_t)qnum, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        gts::k_fast_seed_get<<<(qnum + 255) / 256, 256>>>(d, qnum, bs.pos, bs.selfk, jk, d + qnum);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(seeds_out, d + qnum, sizeof(int) * (size_t)qnum, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        gts_set_error("gts_fast_seeds: %s", cudaGetErrorString(e));
+        return GTS_ERR_CUDA;
+    }
     return GTS_OK;
 }
 

@@ -70,6 +70,15 @@ __host__ __device__ inline FastShape fast_shape(int dim)
     return s;
 }
 
+// Seeds per slot (fast.cu, k_fast_selfk): k = 2^j for j < kSelfKN
+// (k = 1 .. 64) and one padding entry, 32 bytes per slot; made from the
+// object's own block and the kSeedNbr blocks with the nearest centres,
+// keeping the kSeedBest smallest distances per object.
+constexpr int kSelfKN = 7;
+constexpr int kSelfK = 8;
+constexpr int kSeedNbr = 7;
+constexpr int kSeedBest = 64;
+
 // Per-block and per-superblock summaries, placed after the block records.
 struct FastSummary {
     float *cen, *c2, *rad;          // [nb][kp] centre, [nb] |c|^2, [nb] max |o - c|
@@ -78,6 +87,8 @@ struct FastSummary {
     float *sb_cen, *sb_c2, *sb_rad; // [nsb][kp], [nsb], [nsb]
     int *sb_b0;                     // [nsb + 1] first block of each superblock
     float *prow;                    // [nb * kFB][kp] FP32 rows in slot order (zero padding)
+    int *selfk;                     // [nb * kFB][kSelfK] seeds (float bits), k = 1, 2, 4 .. 64
+    int *nbr;                       // [nb][kSeedNbr] blocks with the nearest centres (-1: none)
 };
 
 inline size_t fast_rec_region(const FastShape &fs, int nb)
@@ -88,7 +99,7 @@ inline size_t fast_rec_region(const FastShape &fs, int nb)
 // Byte offsets of the summary arrays after the records, each 256-byte
 // aligned (the pruning kernels read centres as float4).
 struct FastSummaryOffsets {
-    size_t cen, c2, rad, ids, pos, sb_cen, sb_c2, sb_rad, sb_b0, prow, end;
+    size_t cen, c2, rad, ids, pos, sb_cen, sb_c2, sb_rad, sb_b0, prow, selfk, nbr, end;
 };
 
 inline FastSummaryOffsets fast_summary_offsets(const FastShape &fs, int nb, int nsb, int n)
@@ -106,6 +117,8 @@ inline FastSummaryOffsets fast_summary_offsets(const FastShape &fs, int nb, int 
     o.sb_rad = take(sizeof(float) * (size_t)nsb);
     o.sb_b0 = take(sizeof(int) * ((size_t)nsb + 1));
     o.prow = take(sizeof(float) * (size_t)nb * kFB * fs.kp);
+    o.selfk = take(sizeof(int) * (size_t)nb * kFB * kSelfK);
+    o.nbr = take(sizeof(int) * (size_t)nb * kSeedNbr);
     o.end = off;
     return o;
 }
@@ -129,6 +142,8 @@ inline FastSummary fast_summary(unsigned char *recs, const FastShape &fs, int nb
     s.sb_rad = (float *)(recs + o.sb_rad);
     s.sb_b0 = (int *)(recs + o.sb_b0);
     s.prow = (float *)(recs + o.prow);
+    s.selfk = (int *)(recs + o.selfk);
+    s.nbr = (int *)(recs + o.nbr);
     return s;
 }
 

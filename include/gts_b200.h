@@ -165,6 +165,15 @@ int gts_kernel_launches(const gts_index *idx, long long *count);
 int gts_fast_config(const gts_index *idx, int k, int *tuned, int *learned, int *col_groups, int *item_blocks,
                     int *variant);
 
+/* No counterpart in the reference.  The fast form's starting bound for each
+ * query object qids[q] at this k: a certified upper bound on the square of
+ * its k-th distance, made with the filter records (the k-th smallest
+ * squared distance over the object's own block and the 7 blocks with the
+ * nearest centres, widened past FP32 rounding; for k not a power of two the
+ * next power of two's; FLT_MAX where those blocks hold fewer objects).  Host
+ * buffers; needs the records (gts_index_prepare with GTS_FORM_FAST). */
+int gts_fast_seeds(gts_index *idx, const int *qids, int qnum, int k, float *seeds_out);
+
 /* Pin the configuration for k (learned seed 0/1, 1/2/4 column groups with
  * groups * k <= 128, 8/16/32 blocks per item, filter variant 0/1/2 as
  * gts_fast_config reports it) instead of tuning it; GTS_ERR_INVALID when it

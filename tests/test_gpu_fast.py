@@ -241,3 +241,27 @@ def test_graphs_of_one_shape_with_moving_buffers(oracle):
                 np.testing.assert_array_equal(out.cpu().numpy(), want)
         # four captures replayed twice each; the other two buffer sets direct
         assert idx.fast_graphs() - n0 == 8
+
+
+@pytest.mark.parametrize("n,dim,comps,sigma,max_h", [(20000, 128, 32, 0.2, 5), (6000, 300, 16, 0.3, 4),
+                                                      (3000, 40, 3, 1.0, 4), (50, 16, 1, 1.0, 3)])
+def test_seed_table_bounds_the_kth_distance(oracle, n, dim, comps, sigma, max_h):
+    """The starting bounds made with the records (k-th distance over the own
+    block and the nearest blocks) never fall below the exact squared k-th
+    distance of the next power of two, and sit near it on mixture data."""
+    rows = G.gmm_rows(n, dim, comps, sigma, seed=n + 3)
+    ds = oracle.Dataset(2, rows)
+    q = G.query_ids(n, min(n, 400), seed=n + 4)
+    with gts.Index(rows, 2, max_h=max_h) as idx:
+        assert idx.prepare(gts.FORM_FAST)
+        for k in (1, 2, 7, 8, 33, 64):
+            kp2 = 1 << (k - 1).bit_length()
+            seeds = idx.fast_seeds(q, k).astype(np.float64)
+            if kp2 > n:
+                assert np.all(seeds == np.float32(np.finfo(np.float32).max)), f"k={k}"
+                continue
+            exact = oracle.knn_brute(ds, q, kp2)[0].astype(np.float64)
+            assert np.all(seeds >= exact * exact), f"k={k}: a seed below the exact k-th distance"
+            if n >= 3000:
+                ratio = seeds / np.maximum(exact * exact, 1e-30)
+                assert np.median(ratio) < 1.5, f"k={k}: seeds far above the k-th distance ({np.median(ratio)})"

@@ -58,11 +58,15 @@ def test_learned_form_is_exact(oracle, learned_index):
         np.testing.assert_array_equal(dis, bd, err_msg=f"k={k}")
 
 
-def test_learned_radius_gain(learned_index):
-    """What the trained network buys: seeded by min(learned radius, own-block
-    k-th distance), each query starts from a tighter bound than its own block
-    gives, so the filter appends fewer candidates for every k.  Queries the
-    network under-predicts are re-answered (an extra pass) and stay exact."""
+def test_learned_seed_in_the_fast_form(learned_index):
+    """The learned radius as the fast form's seed (min(learned radius, the
+    seed made with the records)): every answer equals the unseeded run's, and
+    queries the network under-predicts are answered again by the next stage
+    (an extra filter pass), never by the plain fallback.  The seed made with
+    the records (k-th distance over the own and seven nearest blocks) is
+    already close to the k-th distance on this data, so here the network
+    adds little to the fast form (the autotuner decides per k); what it
+    gains over the method without it, the GTS traversal, is the next test."""
     rows, idx, info = learned_index
     q = G.query_ids(len(rows), 2000, seed=43)
     with gts.Index(rows, 2, max_h=5) as plain:
@@ -70,17 +74,19 @@ def test_learned_radius_gain(learned_index):
             cg = 4 if k <= 16 else (2 if k <= 32 else 1)
             idx.set_fast_config(k, True, cg)      # the learned seed on, whatever the tuner would pick
             plain.set_fast_config(k, False, cg)
-            idx.knn(q, k, form=gts.FORM_FAST)
+            got = idx.knn(q, k, form=gts.FORM_FAST, return_ids=True)
             learned = idx.search_stats()
-            plain.knn(q, k, form=gts.FORM_FAST)
+            want = plain.knn(q, k, form=gts.FORM_FAST, return_ids=True)
             unlearned = plain.search_stats()
             print(f"k={k} learned: {learned}  unlearned: {unlearned}  train: {info}")
-            assert learned["appended"] < unlearned["appended"], k
+            for x, y in zip(got, want):
+                np.testing.assert_array_equal(x, y, err_msg=f"k={k}")
             assert learned["fallback"] == 0 and unlearned["fallback"] == 0
 
 
 def test_learned_radius_seeds_the_plain_traversal(oracle, learned_index):
-    """GTS_FORM_PLAIN_LEARNED: the GTS traversal starts pruning from the
+    """What the trained network gains over the method without it:
+    GTS_FORM_PLAIN_LEARNED, the GTS traversal starting its pruning from the
     predicted k-th distance instead of from infinity.  Answers equal the
     plain form's (queries whose radius held fewer than k objects are answered
     again unseeded), and fewer leaf objects are read."""
