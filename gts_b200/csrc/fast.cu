@@ -768,7 +768,7 @@ constexpr uint32_t kFTailPad = 1088u;
 
 // Candidates are staged in shared memory during an item; the capacity
 // (a.st_cap) is what the shared memory left after the operands holds.
-constexpr int kFStageMax = 4096;
+constexpr int kFStageMax = 8192;
 
 struct __align__(16) FastCtl {
     uint64_t full[kFS];    // block copy landed
@@ -782,20 +782,14 @@ struct __align__(16) FastCtl {
     int tile, nblk;
     int err;
     int blk[kFItemMax];    // the item's blocks
-    int st_n;              // staged candidates (may run past st_cap: the rest went straight out)
-    int st_cnt[kFT];       // staged candidates per query lane; at the flush: their list offset
+    int th_cnt[4 * kFT];   // at the flush: staged candidates per epilogue thread
+    int qbase[kFT];        // at the flush: list offset per query lane
     int r2s[kFT];          // per query lane: the smallest bound its column groups reached (float bits)
 };
 
-// 12 bytes: the slot (< 2^25) with the query lane in the top 7 bits
-// (all ones: an unused entry), the lower bound, and the lane rank with the
-// margin ub - lb as a half rounded up (so lb + margin >= ub).
-struct FastStaged {
-    uint32_t slot_lane;
-    float lb;
-    uint32_t rank_margin;
-};
-constexpr uint32_t kStagedUnused = 0xffffffffu;
+// A staged candidate: its slot, its lower bound and the margin ub - lb as a
+// half rounded up (so lb + margin >= ub), in three arrays.
+constexpr size_t kStagedBytes = sizeof(int) + sizeof(float) + sizeof(unsigned short);
 
 // Persistent filter kernel, one CTA per SM, 4 x CG epilogue warps + one
 // producer warp.  CG column groups: warps w, w+4, ... share TMEM lanes
@@ -848,8 +842,12 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
     unsigned char *T0 = B0 + (KS ? (size_t)a.nsc * kFChunkBytes : 0);
     unsigned short *heap = reinterpret_cast<unsigned short *>(KS ? T0 + kFS * kFTailPad : B0 + kFS * rec_pad);
     FastCtl &ctl = *reinterpret_cast<FastCtl *>(heap + (KH > 0 ? 0 : NT * a.k));
-    FastStaged *stg = reinterpret_cast<FastStaged *>(&ctl + 1);
-    const int st_cap = a.st_cap;
+    // staging area: a.st_cap entries (slot, lower bound, margin), pcap per
+    // epilogue thread
+    const int st_cap = a.st_cap, pcap = st_cap / NT;
+    int *stg_slot = reinterpret_cast<int *>(&ctl + 1);
+    float *stg_lb = reinterpret_cast<float *>(stg_slot + st_cap);
+    unsigned short *stg_m = reinterpret_cast<unsigned short *>(stg_lb + st_cap);
 
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const bool producer = warp == NEW;
@@ -918,14 +916,11 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
             }
             ctl.tile = tile;
             ctl.nblk = nblk;
-            ctl.st_n = 0;
         }
-        if (t < kFT) {
-            ctl.st_cnt[t] = 0;
-            ctl.r2s[t] = __float_as_int(FLT_MAX);
-        }
+        if (t < kFT) ctl.r2s[t] = __float_as_int(FLT_MAX);
         __syncthreads();
         const int tile = ctl.tile, nblk = ctl.nblk;
+        int nst = 0;   // candidates this (epilogue) thread staged in this item
         if (tile < 0 || ctl.err) break;
         const int4 *tinfo = reinterpret_cast<const int4 *>(a.arec + (size_t)tile * fs.arec_bytes + 2 * fs.atile_bytes);
 
@@ -1173,29 +1168,12 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                         pass &= ~inside;
                         certain += __popc(inside);
                     }
-                    // staging: one shared-memory reservation per warp (prefix
-                    // sum of the lanes' counts), one rank reservation per lane
+                    // staging: each thread appends to its own slice of the
+                    // staging area (entry e of thread t at e * NT + t), no
+                    // atomics; past its slice, straight to the query's list
                     if (!__any_sync(0xffffffffu, pass != 0)) continue;
-                    const int np = __popc(pass);
-                    int incl = np;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                        if (lane >= o) incl += y;
-                    }
-                    const int total = __shfl_sync(0xffffffffu, incl, 31);
-                    int wbase = 0;
-                    if (lane == 31) wbase = atomicAdd(&ctl.st_n, total);
-                    wbase = __shfl_sync(0xffffffffu, wbase, 31);
-                    if (!np) continue;
-                    appended += np;
-                    int at = wbase + incl - np, rank = -1, gsl = 0;
-                    if (at + np <= st_cap) {
-                        rank = atomicAdd(&ctl.st_cnt[lq], np);
-                    } else {
-                        for (int e = at; e < st_cap; e++) stg[e].slot_lane = kStagedUnused;   // reserved, unused
-                        gsl = atomicAdd(&a.cand_cnt[qi], np);
-                    }
+                    if (!pass) continue;
+                    appended += __popc(pass);
 #pragma unroll
                     for (int u = 0; u < 16; u++) {
                         if (!((pass >> u) & 1u)) continue;
@@ -1204,17 +1182,19 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
                         const float lb = T + fmaf(-2.f, __uint_as_float(r[u]), fmaf(-A, dj, wv[jj]));
                         const float ub = lb + 2.f * fmaf(A, dj, eb);
                         const int slot = blk * kFB + jj;
-                        if (rank >= 0) {
-                            const uint32_t mh = __half_as_ushort(__float2half_ru(ub - lb));
-                            stg[at++] = FastStaged{(uint32_t)slot | ((uint32_t)lq << 25), lb, (uint32_t)rank | (mh << 16)};
-                            rank++;
+                        if (nst < pcap) {
+                            const int e = nst * NT + t;
+                            stg_slot[e] = slot;
+                            stg_lb[e] = lb;
+                            stg_m[e] = __half_as_ushort(__float2half_ru(ub - lb));
+                            nst++;
                         } else {
+                            const int gsl = atomicAdd(&a.cand_cnt[qi], 1);
                             if (gsl < kFCand) {
                                 a.cand_pos[(size_t)qi * kFCand + gsl] = slot;
                                 a.cand_lb[(size_t)qi * kFCand + gsl] = lb;
                                 a.cand_ub[(size_t)qi * kFCand + gsl] = ub;
                             }
-                            gsl++;
                         }
                         if (!RANGE && ub < R2) {   // replace the largest of the k kept bounds
                             float mx = -FLT_MAX;
@@ -1273,24 +1253,30 @@ __global__ void __launch_bounds__(128 * CG + 32, 1) k_fast_tile(FastTileArgs a)
         tc_fence_before();
         __syncthreads();   // item done: every MMA consumed, stages and A free
         tc_fence_after();
-        // flush the staged candidates: one list reservation per query lane
+        // flush the staged candidates: one list reservation per query lane,
+        // then each thread writes its own slice after its lane's earlier
+        // column groups
+        if (t < NT) ctl.th_cnt[t] = nst;
+        __syncthreads();
         if (t < kFT) {
-            const int c = ctl.st_cnt[t];
+            int c = 0;
+#pragma unroll
+            for (int g2 = 0; g2 < CG; g2++) c += ctl.th_cnt[t + kFT * g2];
             const int qi = tinfo[t].x;
-            ctl.st_cnt[t] = (c > 0 && qi >= 0) ? atomicAdd(&a.cand_cnt[qi], c) : 0;
+            ctl.qbase[t] = (c > 0 && qi >= 0) ? atomicAdd(&a.cand_cnt[qi], c) : 0;
         }
         __syncthreads();
-        const int ns = min(ctl.st_n, st_cap);
-        for (int e = t; e < ns; e += NT + 32) {
-            const FastStaged v = stg[e];
-            if (v.slot_lane == kStagedUnused) continue;
-            const int l = (int)(v.slot_lane >> 25), qi = tinfo[l].x;
-            const int at = ctl.st_cnt[l] + (int)(v.rank_margin & 0xffffu);
-            if (at < kFCand) {
-                const float margin = __half2float(__ushort_as_half((unsigned short)(v.rank_margin >> 16)));
-                a.cand_pos[(size_t)qi * kFCand + at] = (int)(v.slot_lane & 0x1ffffffu);
-                a.cand_lb[(size_t)qi * kFCand + at] = v.lb;
-                a.cand_ub[(size_t)qi * kFCand + at] = __fadd_ru(v.lb, margin);
+        if (t < NT && nst > 0) {
+            const int qi = tinfo[lq].x;
+            int at = ctl.qbase[lq];
+            for (int g2 = 0; g2 < g; g2++) at += ctl.th_cnt[lq + kFT * g2];
+            for (int e = 0; e < nst && at < kFCand; e++, at++) {
+                const int x = e * NT + t;
+                const float lb = stg_lb[x];
+                const float margin = __half2float(__ushort_as_half(stg_m[x]));
+                a.cand_pos[(size_t)qi * kFCand + at] = stg_slot[x];
+                a.cand_lb[(size_t)qi * kFCand + at] = lb;
+                a.cand_ub[(size_t)qi * kFCand + at] = __fadd_ru(lb, margin);
             }
         }
         __syncthreads();
@@ -1704,13 +1690,15 @@ static int smem_optin()
     return optin;
 }
 
-// K-chunk stages of the streamed form that fit beside at least 4 KB of
-// candidate staging (at most kFSCMax); 0 when not even two fit.
+// K-chunk stages of the streamed form that fit beside candidate staging of
+// at least two entries per epilogue thread (at most kFSCMax); 0 when not
+// even two fit.
 static int fast_tile_stages(const FastShape &fs, int cg, int k, bool heap_in_smem)
 {
     const size_t optin = (size_t)smem_optin();
     for (int nsc = kFSCMax; nsc >= 2; nsc--)
-        if (fast_tile_fixed_smem(fs, cg, k, heap_in_smem, nsc, true) + 4096 <= optin) return nsc;
+        if (fast_tile_fixed_smem(fs, cg, k, heap_in_smem, nsc, true) + 2 * kFT * cg * kStagedBytes <= optin)
+            return nsc;
     return 0;
 }
 
@@ -1720,7 +1708,7 @@ static bool fast_tile_fits(const FastShape &fs, int cg, int k, bool stream)
 {
     const bool heap = k > 16;
     if (fs.kp > kFResKp || stream) return fast_tile_stages(fs, cg, k, heap) >= 2;
-    return fast_tile_fixed_smem(fs, cg, k, heap, 0, false) + 32 * sizeof(FastStaged) <= (size_t)smem_optin();
+    return fast_tile_fixed_smem(fs, cg, k, heap, 0, false) + 2 * kFT * cg * kStagedBytes <= (size_t)smem_optin();
 }
 
 template <int CG, int KH, bool RANGE = false, bool KS = false>
@@ -1735,13 +1723,13 @@ static int launch_fast_tile_cg(const FastTileArgs &a, int grid, cudaStream_t st)
     }
     const size_t fixed = fast_tile_fixed_smem(a.fs, CG, a.k, KH == 0, b.nsc, KS);
     const int optin = smem_optin();
-    b.st_cap = (int)std::min<size_t>(kFStageMax, optin > (int)fixed ? ((size_t)optin - fixed) / sizeof(FastStaged) : 0);
-    b.st_cap &= ~31;
-    if (b.st_cap < 32) {
+    b.st_cap = (int)std::min<size_t>(kFStageMax, optin > (int)fixed ? ((size_t)optin - fixed) / kStagedBytes : 0);
+    b.st_cap -= b.st_cap % (kFT * CG);   // whole slices per epilogue thread
+    if (b.st_cap < kFT * CG) {
         gts_set_error("tensor-core filter: %zu bytes of shared memory leave no room for candidate staging", fixed);
         return GTS_ERR_INVALID;
     }
-    const size_t smem = fixed + sizeof(FastStaged) * (size_t)b.st_cap;
+    const size_t smem = fixed + kStagedBytes * (size_t)b.st_cap;
     GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_tile<CG, KH, RANGE, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
     k_fast_tile<CG, KH, RANGE, KS><<<grid, 128 * CG + 32, smem, st>>>(b);
