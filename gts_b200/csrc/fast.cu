@@ -275,11 +275,12 @@ __global__ void __launch_bounds__(128) k_fast_arec(const float *__restrict__ row
 // k-th smallest distance from the object to the objects of its own block
 // and of the kSeedNbr blocks whose centres lie nearest to its block's (the
 // object itself counts, at distance 0).  Any k of those objects bound the
-// query's k-th distance, and eight blocks hold far more close neighbours
-// than one, so the seed sits much nearer the answer than the own-block
-// k-th distance: fewer blocks survive the pruning and fewer candidates the
-// filter.  Stored for k = 1, 2, 4, .., 64 (a call with another k reads the
-// next power of two: a bound for the larger k bounds every smaller k).
+// query's k-th distance, and 32 blocks (4,096 objects) hold nearly all of
+// a query's close neighbours, so the seed sits next to the answer: at
+// 1,000,000 x 128 and k = 8 the filter lists 9.1 candidates per query
+// against 97 from the own-block k-th distance.  Stored for k = 1, 2, 4, ..,
+// 64 (a call with another k reads the next power of two: a bound for the
+// larger k bounds every smaller k).
 
 // The kSeedNbr blocks with the nearest centres (FP32, ties by block id),
 // -1 where there are fewer blocks.  One warp per block b, eight per CTA;

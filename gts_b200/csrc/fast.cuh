@@ -76,7 +76,7 @@ __host__ __device__ inline FastShape fast_shape(int dim)
 // keeping the kSeedBest smallest distances per object.
 constexpr int kSelfKN = 7;
 constexpr int kSelfK = 8;
-constexpr int kSeedNbr = 7;
+constexpr int kSeedNbr = 31;
 constexpr int kSeedBest = 64;
 
 // Per-block and per-superblock summaries, placed after the block records.

@@ -168,7 +168,7 @@ int gts_fast_config(const gts_index *idx, int k, int *tuned, int *learned, int *
 /* No counterpart in the reference.  The fast form's starting bound for each
  * query object qids[q] at this k: a certified upper bound on the square of
  * its k-th distance, made with the filter records (the k-th smallest
- * squared distance over the object's own block and the 7 blocks with the
+ * squared distance over the object's own block and the 31 blocks with the
  * nearest centres, widened past FP32 rounding; for k not a power of two the
  * next power of two's; FLT_MAX where those blocks hold fewer objects).  Host
  * buffers; needs the records (gts_index_prepare with GTS_FORM_FAST). */

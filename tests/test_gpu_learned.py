@@ -63,7 +63,7 @@ def test_learned_seed_in_the_fast_form(learned_index):
     seed made with the records)): every answer equals the unseeded run's, and
     queries the network under-predicts are answered again by the next stage
     (an extra filter pass), never by the plain fallback.  The seed made with
-    the records (k-th distance over the own and seven nearest blocks) is
+    the records (k-th distance over the own and 31 nearest blocks) is
     already close to the k-th distance on this data, so here the network
     adds little to the fast form (the autotuner decides per k); what it
     gains over the method without it, the GTS traversal, is the next test."""
