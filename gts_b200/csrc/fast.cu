@@ -1809,6 +1809,8 @@ static int fast_prepare(gts_index *idx, cudaStream_t st)
         k_fast_selfk<<<nb, kFB, selfk_smem, st>>>(bs, fs.kp, bs.nbr);
         e = cudaGetLastError();
     }
+    if (e == cudaSuccess && (prune_cop_build(bs.cen, nb, fs, bs.cop, st) || prune_cop_build(bs.sb_cen, nsb, fs, bs.scop, st)))
+        e = cudaErrorUnknown;
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         cudaFree(recs);
@@ -1829,6 +1831,8 @@ static int fast_prepare(gts_index *idx, cudaStream_t st)
 // Buffers of one filter run over qnum queries, carved from a region.
 struct RunBufs {
     int *keys, *vals, *skeys, *order, *cpos, *ccnt, *r2, *ctr, *blist, *bcnt, *heavy;
+    int4 *pitems;   // tensor-core pruning: (tile, block group, mask) items and their count
+    int *pn;
     float *clb, *cub_;
     float *qt;   // [ntiles][kp][128] FP32 query rows of each tile
     unsigned char *arec;
@@ -1882,6 +1886,12 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
     r.blist = (int *)take(4 * (size_t)ntiles * std::max(nb, 1));
     r.bcnt = (int *)take(4 * (size_t)ntiles);
     r.items = (int2 *)take(sizeof(int2) * std::max(itemcap, (size_t)1));
+    r.pitems = nullptr;
+    r.pn = nullptr;
+    if (prune_cop_bytes(fs, nb)) {
+        r.pitems = (int4 *)take(sizeof(int4) * std::max(prune_items_cap(ntiles, nb), (size_t)1));
+        r.pn = (int *)take(8 * sizeof(int));
+    }
     r.cub = take(cub_bytes);
     r.cub_bytes = cub_bytes;
     r.bmask = nullptr;
@@ -1903,6 +1913,40 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
     return off;
 }
 
+// The tiles' needed superblocks, then their needed blocks (blist, bcnt;
+// bmask and bq_cnt for the block-stationary filter): on the tensor cores up
+// to kFResKp (fast_prune.cu), else with the FP32 pruning kernels.
+static int prune_enqueue(gts_index *idx, const FastShape &fs, const FastSummary &bs, const RunBufs &r, int ntiles,
+                         bool blk, cudaStream_t st)
+{
+    const int nb = idx->fast_nb, nsb = idx->fast_nsb, nsbw = (nsb + 31) / 32;
+    if (bs.cop && bs.scop && r.pitems) {
+        int rc = prune_superblocks(r.arec, fs, bs, nsb, ntiles, r.r2, r.sb_mask, nsbw, idx->d_status, st);
+        if (!rc)
+            rc = prune_blocks(r.arec, fs, bs, nb, nsb, ntiles, r.r2, r.sb_mask, nsbw, r.pitems, r.pn, r.blist, r.bcnt,
+                              blk ? r.bmask : nullptr, blk ? r.bq_cnt : nullptr, idx->d_stats, idx->d_status, st);
+        idx->kernel_launches += 3;
+        return rc;
+    }
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const size_t need_smem = need_smem_bytes(fs.kp);
+    GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_sb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
+    GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
+    k_need_sb<<<dim3(ntiles, (nsb + kFChunk - 1) / kFChunk), 256, need_smem, st>>>(r.qt, r.arec, fs, bs, nsb, r.r2,
+                                                                                    r.sb_mask, nsbw);
+    // CTAs per tile: at least kNeedBlkY, more for small batches so that
+    // about four CTAs per SM share the needed superblocks
+    const int need_y = std::max(kNeedBlkY, std::min(32, (4 * nsm + ntiles - 1) / ntiles));
+    k_need_blk<<<dim3(ntiles, need_y), 256, need_smem, st>>>(r.qt, r.arec, fs, bs, r.r2, r.sb_mask, nsbw, r.blist,
+                                                               r.bcnt, nb, idx->d_stats, blk ? r.bmask : nullptr,
+                                                               blk ? r.bq_cnt : nullptr);
+    idx->kernel_launches += 2;
+    GTS_CUDA_TRY(cudaGetLastError());
+    return GTS_OK;
+}
+
 // One filter run over a query batch.  learned: also seed each query's bound
 // from the learned radius model.  carry (nullable): certified starting bounds
 // (float bits, one per query).  Queries the run cannot answer (a learned
@@ -1922,7 +1966,7 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
 {
     const FastShape fs = fast_shape(idx->dim);
     const int ntiles = (qnum + kFT - 1) / kFT;
-    const int nb = idx->fast_nb, nsb = idx->fast_nsb, nsbw = (nsb + 31) / 32;
+    const int nb = idx->fast_nb, nsb = idx->fast_nsb;
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1967,19 +2011,7 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
         GTS_CUDA_TRY(cudaEventRecord(idx->side_ev[1], ss));
         GTS_CUDA_TRY(cudaStreamWaitEvent(st, idx->side_ev[1], 0));
     }
-    const size_t need_smem = need_smem_bytes(fs.kp);
-    GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_sb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
-    GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
-    k_need_sb<<<dim3(ntiles, (nsb + kFChunk - 1) / kFChunk), 256, need_smem, st>>>(
-        r.qt, r.arec, fs, bs, nsb, r.r2, r.sb_mask, nsbw);
-    idx->kernel_launches++;
-    // CTAs per tile: at least kNeedBlkY, more for small batches so that
-    // about four CTAs per SM share the needed superblocks
-    const int need_y = std::max(kNeedBlkY, std::min(32, (4 * nsm + ntiles - 1) / ntiles));
-    k_need_blk<<<dim3(ntiles, need_y), 256, need_smem, st>>>(r.qt, r.arec, fs, bs, r.r2, r.sb_mask, nsbw,
-                                                               r.blist, r.bcnt, nb, idx->d_stats,
-                                                               blk ? r.bmask : nullptr, blk ? r.bq_cnt : nullptr);
-    idx->kernel_launches++;
+    if ((rc = prune_enqueue(idx, fs, bs, r, ntiles, blk, st))) return rc;
     if (!blk) {
         k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, r.bcnt, nb, cfg.item, r.items, r.ctr + 2,
                                                       (int)plan_items_cap(ntiles, nb));
@@ -2616,7 +2648,7 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
     int rc = fast_prepare(idx, st);
     if (rc) return rc;
     const FastShape fs = fast_shape(idx->dim);
-    const int nb = idx->fast_nb, nsb = idx->fast_nsb, nsbw = (nsb + 31) / 32;
+    const int nb = idx->fast_nb, nsb = idx->fast_nsb;
     const bool blk = idx->range_variant == 0 && fast_blk_stages(fs) >= 2;
     auto rbytes_of = [&](int q) { return (plan_run(idx, q, nullptr, nullptr, blk) + 255) & ~(size_t)255; };
     auto ib_of = [&](int q) { return ((size_t)q * sizeof(int) + 255) & ~(size_t)255; };
@@ -2662,15 +2694,7 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
             GTS_CUDA_TRY(cudaMemsetAsync(rb.bq_fill, 0, sizeof(int) * nb, st));
         }
         k_fast_arec<<<ntiles, 128, 0, st>>>(idx->rows, dq, rb.order, n, idx->dim, fs, rb.arec, rb.qt);
-        const size_t need_smem = need_smem_bytes(fs.kp);
-        GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_sb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
-        GTS_CUDA_TRY(cudaFuncSetAttribute(k_need_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_smem));
-        k_need_sb<<<dim3(ntiles, (nsb + kFChunk - 1) / kFChunk), 256, need_smem, st>>>(
-            rb.qt, rb.arec, fs, bs, nsb, rb.r2, rb.sb_mask, nsbw);
-        const int need_y = std::max(kNeedBlkY, std::min(32, (4 * nsm + ntiles - 1) / ntiles));
-        k_need_blk<<<dim3(ntiles, need_y), 256, need_smem, st>>>(rb.qt, rb.arec, fs, bs, rb.r2, rb.sb_mask, nsbw,
-                                                                 rb.blist, rb.bcnt, nb, idx->d_stats,
-                                                                 blk ? rb.bmask : nullptr, blk ? rb.bq_cnt : nullptr);
+        if ((rc = prune_enqueue(idx, fs, bs, rb, ntiles, blk, st))) return rc;
         if (!blk)
             k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, rb.bcnt, nb, 16, rb.items, rb.ctr + 2,
                                                           (int)plan_items_cap(ntiles, nb));

@@ -89,7 +89,16 @@ struct FastSummary {
     float *prow;                    // [nb * kFB][kp] FP32 rows in slot order (zero padding)
     int *selfk;                     // [nb * kFB][kSelfK] seeds (float bits), k = 1, 2, 4 .. 64
     int *nbr;                       // [nb][kSeedNbr] blocks with the nearest centres (-1: none)
+    unsigned char *cop, *scop;      // centre operands of the blocks / superblocks for the tensor-core
+                                    // pruning (fast_prune.cu; null above kFResKp)
 };
+
+// Tensor-core ball pruning (fast_prune.cu), padded dimension <= kFResKp:
+// bytes of a centre operand of n balls (0 above kFResKp), and its build
+// from FP32 centres ([n][kp]).
+size_t prune_cop_bytes(const FastShape &fs, int n);
+int prune_cop_build(const float *cen, int n, const FastShape &fs, unsigned char *cop, cudaStream_t st);
+size_t prune_items_cap(int ntiles, int nb);
 
 inline size_t fast_rec_region(const FastShape &fs, int nb)
 {
@@ -99,7 +108,7 @@ inline size_t fast_rec_region(const FastShape &fs, int nb)
 // Byte offsets of the summary arrays after the records, each 256-byte
 // aligned (the pruning kernels read centres as float4).
 struct FastSummaryOffsets {
-    size_t cen, c2, rad, ids, pos, sb_cen, sb_c2, sb_rad, sb_b0, prow, selfk, nbr, end;
+    size_t cen, c2, rad, ids, pos, sb_cen, sb_c2, sb_rad, sb_b0, prow, selfk, nbr, cop, scop, end;
 };
 
 inline FastSummaryOffsets fast_summary_offsets(const FastShape &fs, int nb, int nsb, int n)
@@ -119,6 +128,8 @@ inline FastSummaryOffsets fast_summary_offsets(const FastShape &fs, int nb, int 
     o.prow = take(sizeof(float) * (size_t)nb * kFB * fs.kp);
     o.selfk = take(sizeof(int) * (size_t)nb * kFB * kSelfK);
     o.nbr = take(sizeof(int) * (size_t)nb * kSeedNbr);
+    o.cop = take(prune_cop_bytes(fs, nb));
+    o.scop = take(prune_cop_bytes(fs, nsb));
     o.end = off;
     return o;
 }
@@ -144,8 +155,20 @@ inline FastSummary fast_summary(unsigned char *recs, const FastShape &fs, int nb
     s.prow = (float *)(recs + o.prow);
     s.selfk = (int *)(recs + o.selfk);
     s.nbr = (int *)(recs + o.nbr);
+    s.cop = prune_cop_bytes(fs, nb) ? recs + o.cop : nullptr;
+    s.scop = prune_cop_bytes(fs, nsb) ? recs + o.scop : nullptr;
     return s;
 }
+
+// The tiles' needed superblocks (mask words sb_mask[tile][nsbw]) and then
+// their needed blocks (appended to blist[tile][nb], counts in bcnt; with
+// bmask, each block's lanes and pairs per block in bq_cnt), on the tensor
+// cores (fast_prune.cu).
+int prune_superblocks(const unsigned char *arec, const FastShape &fs, const FastSummary &bs, int nsb, int ntiles,
+                      const int *r2_bits, uint32_t *sb_mask, int nsbw, int *status, cudaStream_t st);
+int prune_blocks(const unsigned char *arec, const FastShape &fs, const FastSummary &bs, int nb, int nsb, int ntiles,
+                 const int *r2_bits, const uint32_t *sb_mask, int nsbw, int4 *items, int *n_items, int *blist,
+                 int *bcnt, uint4 *bmask, int *bq_cnt, unsigned long long *stats, int *status, cudaStream_t st);
 
 // Result of the order construction, in the index's scratch: positions of
 // the final order (perm: position -> object id), the blocks as position

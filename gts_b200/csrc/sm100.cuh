@@ -150,6 +150,19 @@ __device__ __forceinline__ void tmem_wait_ld(uint32_t (&r)[16])
                  : "memory");
 }
 
+// Keeps uses of r after this point: with tmem_wait_ld on another array of the
+// same batch of loads, every register of r is complete here (the wait covers
+// all of the thread's loads in flight).
+__device__ __forceinline__ void reg_fence(uint32_t (&r)[16])
+{
+    asm volatile(""
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15])
+                 :
+                 : "memory");
+}
+
 // ---------------------------------------------------------------- MMA
 
 // Shared-memory matrix descriptor: K-major operand in the 128-byte swizzled
