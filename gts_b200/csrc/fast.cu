@@ -233,39 +233,61 @@ __global__ void __launch_bounds__(256) k_fast_sbprep(int dim, const float *__res
 
 // One CTA per tile: the A operand of the tile's 128 queries (sorted by block
 // order), split into BF16 hi + lo, in the swizzled layout, and per lane
-// (query index, |q|^2, |q|).  A tile record is one bulk copy.  Beside it an
-// FP32 copy of the rows ([kp][128], zero padding) for the pruning kernels.
+// (query index, |q|^2, |q|).  A tile record is one bulk copy.  With qt, beside
+// it an FP32 copy of the rows ([kp][128], zero padding) for the FP32 pruning
+// kernels.  The tile's rows pass through shared memory 64 columns at a time:
+// the CTA reads them coalesced (a warp reads 32 consecutive values of one
+// row, all of a thread's loads in flight at once), then each thread converts
+// its own query's row; |q|^2 is summed in column order as before.
 __global__ void __launch_bounds__(128) k_fast_arec(const float *__restrict__ rows, const int *__restrict__ qids,
                                                    const int *__restrict__ order, int qnum, int dim, FastShape fs,
                                                    unsigned char *__restrict__ arec, float *__restrict__ qt)
 {
-    float *qtt = qt + (size_t)blockIdx.x * fs.kp * kFT;
+    __shared__ float sx[kFT][64 + 1];
+    __shared__ int rid[kFT];
     const int tile = blockIdx.x, lq = threadIdx.x;
+    float *qtt = qt ? qt + (size_t)blockIdx.x * fs.kp * kFT : nullptr;
     unsigned char *A_hi = arec + (size_t)tile * fs.arec_bytes, *A_lo = A_hi + fs.atile_bytes;
     int4 *info = reinterpret_cast<int4 *>(A_lo + fs.atile_bytes);
     const int slot = tile * kFT + lq;
     const int qi = slot < qnum ? order[slot] : -1;
-    const float *row = qi >= 0 ? rows + (size_t)qids[qi] * dim : nullptr;
+    rid[lq] = qi >= 0 ? qids[qi] : -1;
+    __syncthreads();
     double acc = 0.0;
-    for (int j0 = 0; j0 < fs.kp; j0 += 8) {
-        unsigned short hi[8], lo[8];
+    for (int c0 = 0; c0 < fs.kp; c0 += 64) {
+        float v[64];
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            int j = j0 + u;
-            float x = (row && j < dim) ? row[j] : 0.f;
-            qtt[(size_t)j * kFT + lq] = x;
-            acc += (double)x * x;
-            hi[u] = f2bf(x);
-            lo[u] = f2bf(x - bf2f(hi[u]));
+        for (int m = 0; m < 64; m++) {
+            const int i = lq + 128 * m, r = i >> 6, j = c0 + (i & 63);
+            const int id = rid[r];
+            v[m] = (id >= 0 && j < dim) ? rows[(size_t)id * dim + j] : 0.f;
         }
-        uint4 vh, vl;
-        vh.x = hi[0] | ((uint32_t)hi[1] << 16); vh.y = hi[2] | ((uint32_t)hi[3] << 16);
-        vh.z = hi[4] | ((uint32_t)hi[5] << 16); vh.w = hi[6] | ((uint32_t)hi[7] << 16);
-        vl.x = lo[0] | ((uint32_t)lo[1] << 16); vl.y = lo[2] | ((uint32_t)lo[3] << 16);
-        vl.z = lo[4] | ((uint32_t)lo[5] << 16); vl.w = lo[6] | ((uint32_t)lo[7] << 16);
-        uint32_t off = sw128_offset(lq, j0, kFT);
-        *reinterpret_cast<uint4 *>(A_hi + off) = vh;
-        *reinterpret_cast<uint4 *>(A_lo + off) = vl;
+#pragma unroll
+        for (int m = 0; m < 64; m++) {
+            const int i = lq + 128 * m;
+            sx[i >> 6][i & 63] = v[m];
+        }
+        __syncthreads();
+        for (int j0 = 0; j0 < 64; j0 += 8) {
+            unsigned short hi[8], lo[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const float x = sx[lq][j0 + u];
+                if (qtt) qtt[(size_t)(c0 + j0 + u) * kFT + lq] = x;
+                acc += (double)x * x;
+                hi[u] = f2bf(x);
+                lo[u] = f2bf(x - bf2f(hi[u]));
+            }
+            uint4 vh, vl;
+            vh.x = hi[0] | ((uint32_t)hi[1] << 16); vh.y = hi[2] | ((uint32_t)hi[3] << 16);
+            vh.z = hi[4] | ((uint32_t)hi[5] << 16); vh.w = hi[6] | ((uint32_t)hi[7] << 16);
+            vl.x = lo[0] | ((uint32_t)lo[1] << 16); vl.y = lo[2] | ((uint32_t)lo[3] << 16);
+            vl.z = lo[4] | ((uint32_t)lo[5] << 16); vl.w = lo[6] | ((uint32_t)lo[7] << 16);
+            const uint32_t off = sw128_offset(lq, c0 + j0, kFT);
+            *reinterpret_cast<uint4 *>(A_hi + off) = vh;
+            *reinterpret_cast<uint4 *>(A_lo + off) = vl;
+        }
+        __syncthreads();
     }
     info[lq] = make_int4(qi, __float_as_int((float)acc), __float_as_int((float)sqrt(acc)), 0);
 }
@@ -1579,6 +1601,173 @@ __global__ void __launch_bounds__(128) k_fast_final(const float *__restrict__ ro
 
 // Sort keys of the queries: the block of their slot (tiles group queries
 // by block order; the order inside a block does not matter).
+// Light recheck, one warp per query, for small k (where nearly every query
+// lists at most 32 candidates), so a query needs no CTA barrier and a CTA
+// runs kFinWarps queries side by side.  The tests and the arithmetic are
+// k_fast_final's: the bound drops to the k-th smallest upper bound; each
+// candidate within it gets its reference value (exact squares first; pow
+// where a value lies near a float rounding midpoint, another value or the
+// bound); ranks by (distance, id).  FB candidates at a time, the warp reads
+// their rows coalesced (all loads in flight at once) and keeps the FP32
+// differences o_j - q_j in shared memory; lane p then sums candidate p's
+// terms in j order.  Queries with more than 32 candidates go to `heavy`
+// (the full variant of k_fast_final), those whose list overflowed to
+// `overflow`.
+constexpr int kFinWarps = 4;
+constexpr int kFinWarpK = 8;   // k up to which the warp variant runs first
+template <int KPM, int FB>
+__global__ void __launch_bounds__(32 * kFinWarps) k_fast_final_warp(
+    const float *__restrict__ rows, int dim, int num, const float *__restrict__ prow, int kp,
+    const int *__restrict__ ids_of_slot, int nslots, const int *__restrict__ qids, int qnum, int k, int infi_dis,
+    const int *__restrict__ cand_pos, const float *__restrict__ cand_lb, const float *__restrict__ cand_ub,
+    const int *__restrict__ cand_cnt, const int *__restrict__ r2_bits, float *kth, int *ids, float *dists,
+    int *overflow, int *n_overflow, int *heavy, int *n_heavy, unsigned long long *stats)
+{
+    __shared__ float ew_all[kFinWarps][FB][KPM + 1];   // +1: lane p's reads of column j miss each other's banks
+    __shared__ int wslot[kFinWarps][32], wid[kFinWarps][32];
+    __shared__ unsigned long long nrechk;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float(*ew)[KPM + 1] = ew_all[warp];
+    if (threadIdx.x == 0) nrechk = 0;
+    __syncthreads();
+    const int q = blockIdx.x * kFinWarps + warp;
+    const int cnt = q < qnum ? cand_cnt[q] : 0;
+    if (q < qnum && cnt > 32) {
+        if (lane == 0) {
+            if (cnt <= kFCand) heavy[atomicAdd(n_heavy, 1)] = q;
+            else overflow[atomicAdd(n_overflow, 1)] = q;
+        }
+    } else if (q < qnum) {
+        const int qid = qids[q];
+        float R2 = __int_as_float(r2_bits[q]);
+        const bool have = lane < cnt;
+        const size_t cb = (size_t)q * kFCand + lane;
+        const float ub = have ? cand_ub[cb] : INFINITY;
+        const float lb = have ? cand_lb[cb] : INFINITY;
+        const int slot = have ? cand_pos[cb] : -1;
+        // the query's row, lane l holding columns l, l + 32, ..
+        const float *qrow = rows + (size_t)qid * dim;
+        float qv[KPM / 32];
+#pragma unroll
+        for (int m = 0; m < KPM / 32; m++) {
+            const int j = lane + 32 * m;
+            qv[m] = j < dim ? qrow[j] : 0.f;
+        }
+        if (cnt >= k) {
+            // k-th smallest upper bound (with multiplicity): the lane of rank k - 1
+            int rank = 0;
+            for (int j = 0; j < 32; j++) {
+                const float uj = __shfl_sync(0xffffffffu, ub, j);
+                rank += (uj < ub) || (uj == ub && j < lane);
+            }
+            const unsigned who = __ballot_sync(0xffffffffu, have && rank == k - 1);
+            R2 = fminf(R2, __shfl_sync(0xffffffffu, ub, __ffs(who) - 1));
+        }
+        bool c = have && !(lb > R2) && slot >= 0 && slot < nslots;
+        int id = -1;
+        if (c) {
+            id = ids_of_slot[slot];
+            c = id >= 0 && id < num;
+        }
+        // candidates packed: lane p < n holds the p-th
+        const unsigned cm = __ballot_sync(0xffffffffu, c);
+        const int n = __popc(cm);
+        if (c) {
+            const int p = __popc(cm & ((1u << lane) - 1u));
+            wslot[warp][p] = slot;
+            wid[warp][p] = id;
+        }
+        __syncwarp();
+        const bool mine = lane < n;
+        const int pid = mine ? wid[warp][lane] : 0x7fffffff;
+        const double lim = (double)R2 * (1.0 - 1e-6);
+        double d = DBL_MAX;
+        for (int pass = 0; pass < 2; pass++) {
+            double r = 0.0;
+            for (int b0 = 0; b0 < n; b0 += FB) {
+                const int nbat = min(FB, n - b0);
+                float e[FB][KPM / 32];
+#pragma unroll
+                for (int cc = 0; cc < FB; cc++) {
+                    const float *orow = prow + (size_t)(cc < nbat ? wslot[warp][b0 + cc] : 0) * kp;
+#pragma unroll
+                    for (int m = 0; m < KPM / 32; m++) {
+                        const int j = lane + 32 * m;
+                        e[cc][m] = (cc < nbat && j < dim) ? orow[j] : 0.f;
+                    }
+                }
+#pragma unroll
+                for (int cc = 0; cc < FB; cc++)
+#pragma unroll
+                    for (int m = 0; m < KPM / 32; m++) ew[cc][lane + 32 * m] = e[cc][m] - qv[m];
+                __syncwarp();
+                if (lane >= b0 && lane < b0 + nbat) {
+                    const float *er = ew[lane - b0];
+                    if (pass == 0) {
+                        // a float difference squared is exact in FP64
+#pragma unroll 8
+                        for (int j = 0; j < dim; j++) {
+                            const double x = (double)er[j];
+                            r += x * x;
+                        }
+                    } else {
+                        for (int j = 0; j < dim; j++) {
+                            const double tj = pow(er[j], 2);
+                            r += tj;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            if (mine) d = pid == qid ? 0.0 : pow(r, 0.5);
+            if (pass == 1) break;
+            bool rk = false;
+            if (mine && d != 0.0) {
+                // the float midpoints around (float)d must stay beyond delta
+                const float f = __double2float_rn(d);
+                const double fd = f;
+                const double mhi = 0.5 * (fd + (double)__int_as_float(__float_as_int(f) + 1));
+                const double mlo = 0.5 * (fd + (double)__int_as_float(__float_as_int(f) - 1));
+                const double dl = d * 1e-13;
+                const double v2 = d * d;
+                if (!(f > 0.f && d - dl > mlo && d + dl < mhi) || fabs(v2 - lim) <= 3e-13 * lim) rk = true;
+            }
+            // near-ties: two values closer than their margins (exact zeros are
+            // exact in both sums)
+            for (int j = 0; j < n; j++) {
+                const double dj = __shfl_sync(0xffffffffu, d, j);
+                if (mine && j != lane && !(d == 0.0 && dj == 0.0) && fabs(dj - d) <= (d + dj) * 1e-13) rk = true;
+            }
+            if (!__any_sync(0xffffffffu, rk)) break;
+        }
+        if (lane == 0 && n) atomicAdd(&nrechk, (unsigned long long)n);
+        int rank = 0;
+        for (int j = 0; j < n; j++) {
+            const double dj = __shfl_sync(0xffffffffu, d, j);
+            const int ij = __shfl_sync(0xffffffffu, pid, j);
+            rank += (dj < d) || (dj == d && ij < pid);
+        }
+        const bool top = mine && rank < k;
+        const int within = __popc(__ballot_sync(0xffffffffu, top && d * d <= lim));
+        if (within < k && within < num) {
+            if (lane == 0) overflow[atomicAdd(n_overflow, 1)] = q;
+        } else {
+            if (top) {
+                if (ids) ids[(size_t)q * k + rank] = pid;
+                if (dists) dists[(size_t)q * k + rank] = (float)d;
+                if (rank == k - 1) kth[q] = (float)d;
+            }
+            for (int j = n + lane; j < k; j += 32) {
+                if (ids) ids[(size_t)q * k + j] = -1;
+                if (dists) dists[(size_t)q * k + j] = (float)infi_dis;
+            }
+            if (n < k && lane == 0) kth[q] = (float)infi_dis;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && stats && nrechk) atomicAdd(&stats[2], nrechk);
+}
+
 __global__ void k_fast_keys(const int *qids, int qnum, const int *pos_of, int *keys, int *vals)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1635,21 +1824,25 @@ static int fast_cg(int k) { return k <= 32 ? 4 : 2; }
 // epilogue column groups (warps per query lane), blocks per work item,
 // records streamed in K chunks (forced above kp = kFResKp) or resident --
 // or the block-stationary filter (blk; fast_blk.cu), which has no column
-// groups or items.
+// groups or items.  wfin: the light recheck one warp per query
+// (k_fast_final_warp, k <= kFinWarpK) instead of one CTA per query.
 struct FastCfg {
     bool learned;
     int cg, item;
     bool stream;
     bool blk;
+    bool wfin;
 };
 
 static int cfg_pack(const FastCfg &c)
 {
-    return 1 | (c.learned ? 2 : 0) | (c.cg << 2) | (c.item << 8) | (c.stream ? 1 << 14 : 0) | (c.blk ? 1 << 15 : 0);
+    return 1 | (c.learned ? 2 : 0) | (c.cg << 2) | (c.item << 8) | (c.stream ? 1 << 14 : 0) | (c.blk ? 1 << 15 : 0) |
+           (c.wfin ? 1 << 16 : 0);
 }
 static FastCfg cfg_unpack(int v)
 {
-    return FastCfg{(v & 2) != 0, (v >> 2) & 7, (v >> 8) & 63, (v & (1 << 14)) != 0, (v & (1 << 15)) != 0};
+    return FastCfg{(v & 2) != 0, (v >> 2) & 7, (v >> 8) & 63, (v & (1 << 14)) != 0, (v & (1 << 15)) != 0,
+                   (v & (1 << 16)) != 0};
 }
 
 // Filter variant of a configuration as the ABI reports it.
@@ -1831,8 +2024,7 @@ static int fast_prepare(gts_index *idx, cudaStream_t st)
 // Buffers of one filter run over qnum queries, carved from a region.
 struct RunBufs {
     int *keys, *vals, *skeys, *order, *cpos, *ccnt, *r2, *ctr, *blist, *bcnt, *heavy;
-    int4 *pitems;   // tensor-core pruning: (tile, block group, mask) items and their count
-    int *pn;
+    unsigned char *pbufs;   // tensor-core pruning: the block pass's items and result words
     float *clb, *cub_;
     float *qt;   // [ntiles][kp][128] FP32 query rows of each tile
     unsigned char *arec;
@@ -1882,16 +2074,14 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
     r.heavy = (int *)take(4 * (size_t)qnum);
     r.arec = take((size_t)ntiles * fs.arec_bytes);
     r.sb_mask = (uint32_t *)take(4 * (size_t)ntiles * std::max(nsbw, 1));
-    r.qt = (float *)take(4 * (size_t)ntiles * fs.kp * kFT);
+    // the FP32 tile rows serve only the FP32 pruning kernels (no tensor-core pruning)
+    const bool tc_prune = prune_cop_bytes(fs, nb) && prune_cop_bytes(fs, idx->fast_nsb);
+    r.qt = tc_prune ? nullptr : (float *)take(4 * (size_t)ntiles * fs.kp * kFT);
     r.blist = (int *)take(4 * (size_t)ntiles * std::max(nb, 1));
     r.bcnt = (int *)take(4 * (size_t)ntiles);
     r.items = (int2 *)take(sizeof(int2) * std::max(itemcap, (size_t)1));
-    r.pitems = nullptr;
-    r.pn = nullptr;
-    if (prune_cop_bytes(fs, nb)) {
-        r.pitems = (int4 *)take(sizeof(int4) * std::max(prune_items_cap(ntiles, nb), (size_t)1));
-        r.pn = (int *)take(8 * sizeof(int));
-    }
+    const bool lanes = blk && fast_blk_stages(fs) >= 2;   // the block-stationary filter's lane masks
+    r.pbufs = tc_prune ? take(prune_block_bufs(ntiles, nb, lanes)) : nullptr;
     r.cub = take(cub_bytes);
     r.cub_bytes = cub_bytes;
     r.bmask = nullptr;
@@ -1920,12 +2110,12 @@ static int prune_enqueue(gts_index *idx, const FastShape &fs, const FastSummary 
                          bool blk, cudaStream_t st)
 {
     const int nb = idx->fast_nb, nsb = idx->fast_nsb, nsbw = (nsb + 31) / 32;
-    if (bs.cop && bs.scop && r.pitems) {
+    if (bs.cop && bs.scop && r.pbufs) {
         int rc = prune_superblocks(r.arec, fs, bs, nsb, ntiles, r.r2, r.sb_mask, nsbw, idx->d_status, st);
         if (!rc)
-            rc = prune_blocks(r.arec, fs, bs, nb, nsb, ntiles, r.r2, r.sb_mask, nsbw, r.pitems, r.pn, r.blist, r.bcnt,
+            rc = prune_blocks(r.arec, fs, bs, nb, ntiles, r.r2, r.sb_mask, nsbw, r.pbufs, r.blist, r.bcnt,
                               blk ? r.bmask : nullptr, blk ? r.bq_cnt : nullptr, idx->d_stats, idx->d_status, st);
-        idx->kernel_launches += 3;
+        idx->kernel_launches += 4;
         return rc;
     }
     int dev = 0, nsm = 148;
@@ -2101,7 +2291,31 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
             per_sm = 4;
         return std::min(qnum, per_sm * nsm);
     };
-    if (fs.kp <= kFResKp) {
+    if (cfg.wfin && k <= kFinWarpK) {
+        // one warp per query; lists over 32 candidates to the full variant
+        if (fs.kp <= kFResKp)
+            k_fast_final_warp<kFResKp, 8><<<(qnum + kFinWarps - 1) / kFinWarps, 32 * kFinWarps, 0, st>>>(
+                idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, qnum, k,
+                idx->params.infi_dis, r.cpos, r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr,
+                r.heavy, r.ctr + 4, idx->d_stats);
+        else
+            k_fast_final_warp<kFMaxKp, 2><<<(qnum + kFinWarps - 1) / kFinWarps, 32 * kFinWarps, 0, st>>>(
+                idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, qnum, k,
+                idx->params.infi_dis, r.cpos, r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr,
+                r.heavy, r.ctr + 4, idx->d_stats);
+        if (fs.kp <= kFResKp)
+            k_fast_final<kFResKp, kFinB, kFCand><<<full_grid((const void *)k_fast_final<kFResKp, kFinB, kFCand>), 128,
+                                                    0, st>>>(
+                idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis,
+                r.cpos, r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, nullptr, nullptr, r.heavy,
+                r.ctr + 4, idx->d_stats);
+        else
+            k_fast_final<kFMaxKp, kFinB / 2, kFCand><<<
+                full_grid((const void *)k_fast_final<kFMaxKp, kFinB / 2, kFCand>), 128, 0, st>>>(
+                idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis,
+                r.cpos, r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, nullptr, nullptr, r.heavy,
+                r.ctr + 4, idx->d_stats);
+    } else if (fs.kp <= kFResKp) {
         k_fast_final<kFResKp, kFinB, 128><<<qnum, 128, 0, st>>>(
             idx->rows, idx->dim, idx->num, bs.prow, fs.kp, bs.ids, nb * kFB, d_qids, k, idx->params.infi_dis, r.cpos,
             r.clb, r.cub_, r.ccnt, r.r2, d_kth, d_ids, d_dists, d_fail, r.ctr, r.heavy, r.ctr + 4, nullptr, nullptr,
@@ -2414,7 +2628,8 @@ static int fast_autotune(gts_index *idx, FastCall &fc, int qc, const int *d_qids
                         cands.push_back(FastCfg{learned != 0, cg, item, stream != 0, false});
         }
     }
-    for (const FastCfg &c : cands) {
+    for (size_t ci = 0; ci < cands.size(); ci++) {
+        const FastCfg c = cands[ci];
         if (cudaEventRecord(e0, st) != cudaSuccess) {
             rc = GTS_ERR_CUDA;
             break;
@@ -2429,6 +2644,12 @@ static int fast_autotune(gts_index *idx, FastCall &fc, int qc, const int *d_qids
         if (ms < best_ms) {
             best_ms = ms;
             best = c;
+        }
+        // after the filter configurations, the best one with the other light recheck
+        if (ci + 1 == cands.size() && k <= kFinWarpK && !best.wfin) {
+            FastCfg w = best;
+            w.wfin = true;
+            cands.push_back(w);
         }
     }
     cudaEventDestroy(e0);
