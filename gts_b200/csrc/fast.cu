@@ -1777,13 +1777,31 @@ __global__ void k_fast_keys(const int *qids, int qnum, const int *pos_of, int *k
     }
 }
 
-__global__ void k_fast_init(int qnum, int *cand_cnt, int *r2_bits, const int *carry)
+// The start of a kNN filter run in one launch.  Per query i: an empty
+// candidate list, the starting bound (carry, else FLT_MAX; with selfk, the
+// smaller of that and the seed table's bound for the k at column jk) and the
+// sort key (the block of the query's slot) with its index; over the grid:
+// the run's counters, the tiles' block counts and the superblock mask words
+// cleared, and the run counted in stats[6].
+__global__ void k_fast_begin(int qnum, const int *__restrict__ qids, const int *__restrict__ pos_of,
+                             const int *__restrict__ selfk, int jk, const int *__restrict__ carry, int *cand_cnt,
+                             int *r2_bits, int *keys, int *vals, int *ctr, int nctr, int *bcnt, int ntiles,
+                             uint32_t *sb_mask, int nmask, unsigned long long *stats)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
     if (i < qnum) {
+        const int pos = pos_of[qids[i]];
+        int r2 = carry ? carry[i] : __float_as_int(FLT_MAX);
+        if (selfk) r2 = min(r2, selfk[(size_t)pos * kSelfK + jk]);   // non-negative floats order as ints
         cand_cnt[i] = 0;
-        r2_bits[i] = carry ? carry[i] : __float_as_int(FLT_MAX);
+        r2_bits[i] = r2;
+        keys[i] = pos / kFB;
+        vals[i] = i;
     }
+    if (i < nctr) ctr[i] = 0;
+    for (int j = i; j < ntiles; j += stride) bcnt[j] = 0;
+    for (int j = i; j < nmask; j += stride) sb_mask[j] = 0u;
+    if (i == 0 && stats) stats[6] += 1ull;
 }
 
 __global__ void k_add_stat(unsigned long long *p, unsigned long long v) { *p += v; }
@@ -2105,17 +2123,23 @@ static size_t plan_run(const gts_index *idx, int qnum, unsigned char *base, RunB
 
 // The tiles' needed superblocks, then their needed blocks (blist, bcnt;
 // bmask and bq_cnt for the block-stationary filter): on the tensor cores up
-// to kFResKp (fast_prune.cu), else with the FP32 pruning kernels.
+// to kFResKp (fast_prune.cu), else with the FP32 pruning kernels.  cleared:
+// the superblock masks are zero already.  item > 0: the tensor-core path
+// also makes the tile filter's work items of `item` blocks (*listed = true);
+// otherwise the caller runs k_items.
 static int prune_enqueue(gts_index *idx, const FastShape &fs, const FastSummary &bs, const RunBufs &r, int ntiles,
-                         bool blk, cudaStream_t st)
+                         bool blk, bool cleared, int item, bool *listed, cudaStream_t st)
 {
     const int nb = idx->fast_nb, nsb = idx->fast_nsb, nsbw = (nsb + 31) / 32;
+    *listed = false;
     if (bs.cop && bs.scop && r.pbufs) {
-        int rc = prune_superblocks(r.arec, fs, bs, nsb, ntiles, r.r2, r.sb_mask, nsbw, idx->d_status, st);
+        int rc = prune_superblocks(r.arec, fs, bs, nsb, ntiles, r.r2, r.sb_mask, nsbw, !cleared, idx->d_status, st);
         if (!rc)
-            rc = prune_blocks(r.arec, fs, bs, nb, ntiles, r.r2, r.sb_mask, nsbw, r.pbufs, r.blist, r.bcnt,
-                              blk ? r.bmask : nullptr, blk ? r.bq_cnt : nullptr, idx->d_stats, idx->d_status, st);
+            rc = prune_blocks(r.arec, fs, bs, nb, ntiles, r.r2, r.sb_mask, nsbw, r.pbufs, r.ctr + 5, r.blist, r.bcnt,
+                              blk ? r.bmask : nullptr, blk ? r.bq_cnt : nullptr, item, item > 0 ? r.items : nullptr,
+                              r.ctr + 2, (int)plan_items_cap(ntiles, nb), idx->d_stats, idx->d_status, st);
         idx->kernel_launches += 4;
+        *listed = item > 0;
         return rc;
     }
     int dev = 0, nsm = 148;
@@ -2163,33 +2187,28 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     int rc;
     const FastSummary bs = fast_summary(idx->fast_recs, fs, nb, nsb, idx->num);
 
-    k_fast_init<<<(qnum + 255) / 256, 256, 0, st>>>(qnum, r.ccnt, r.r2, carry);
-    idx->kernel_launches++;
-    if (learned && (rc = mlp_seed(idx, d_qids, qnum, k, r.r2, st))) return rc;
-    // the certified own-block seed (with a learned radius the smaller of the
-    // two is used, and queries it under-predicts are answered again), on the
-    // side stream when the handle has one: it needs only the bounds, while
-    // the query sort and the tile operands proceed on st (inside a capture
-    // the two become parallel branches of the graph)
-    cudaStream_t ss = idx->side_stream ? idx->side_stream : st;
-    if (ss != st) {
-        GTS_CUDA_TRY(cudaEventRecord(idx->side_ev[0], st));
-        GTS_CUDA_TRY(cudaStreamWaitEvent(ss, idx->side_ev[0], 0));
-    }
     int jk = 0;   // the table's k: the smallest power of two >= k (k <= kFMaxK = 2^(kSelfKN - 1))
     while ((1 << jk) < k) jk++;
-    k_fast_seed_tab<<<(qnum + 255) / 256, 256, 0, ss>>>(d_qids, qnum, bs.pos, bs.selfk, jk, r.r2);
+    // per-query start, counters and masks cleared, in one launch; with a
+    // learned radius its prediction replaces the start bound and the table's
+    // bound is applied after it (the smaller of the two is used, and queries
+    // it under-predicts are answered again)
+    const int nsbw = (idx->fast_nsb + 31) / 32;
+    k_fast_begin<<<(qnum + 255) / 256, 256, 0, st>>>(qnum, d_qids, bs.pos, learned ? nullptr : bs.selfk, jk, carry,
+                                                     r.ccnt, r.r2, r.keys, r.vals, r.ctr, 8, r.bcnt, ntiles, r.sb_mask,
+                                                     ntiles * nsbw, idx->d_stats);
     idx->kernel_launches++;
-    k_fast_keys<<<(qnum + 255) / 256, 256, 0, st>>>(d_qids, qnum, bs.pos, r.keys, r.vals);
-    idx->kernel_launches++;
+    if (learned) {
+        if ((rc = mlp_seed(idx, d_qids, qnum, k, r.r2, st))) return rc;
+        k_fast_seed_tab<<<(qnum + 255) / 256, 256, 0, st>>>(d_qids, qnum, bs.pos, bs.selfk, jk, r.r2);
+        idx->kernel_launches++;
+    }
     // block ids are below nb: sort only the bits they use
     int key_bits = 1;
     while (key_bits < 32 && (1ll << key_bits) < (long long)nb) key_bits++;
     size_t cb = r.cub_bytes;
     GTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(r.cub, cb, r.keys, r.skeys, r.vals, r.order, qnum, 0, key_bits,
                                                  st));
-    GTS_CUDA_TRY(cudaMemsetAsync(r.ctr, 0, 8 * sizeof(int), st));
-    GTS_CUDA_TRY(cudaMemsetAsync(r.bcnt, 0, sizeof(int) * ntiles, st));
     const bool blk = cfg.blk && r.bmask && fast_blk_stages(fs) >= 2;
     if (blk) {
         GTS_CUDA_TRY(cudaMemsetAsync(r.bq_cnt, 0, sizeof(int) * nb, st));
@@ -2197,12 +2216,9 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
     }
     k_fast_arec<<<ntiles, 128, 0, st>>>(idx->rows, d_qids, r.order, qnum, idx->dim, fs, r.arec, r.qt);
     idx->kernel_launches++;
-    if (ss != st) {
-        GTS_CUDA_TRY(cudaEventRecord(idx->side_ev[1], ss));
-        GTS_CUDA_TRY(cudaStreamWaitEvent(st, idx->side_ev[1], 0));
-    }
-    if ((rc = prune_enqueue(idx, fs, bs, r, ntiles, blk, st))) return rc;
-    if (!blk) {
+    bool listed = false;   // the filter's work items already made by the pruning
+    if ((rc = prune_enqueue(idx, fs, bs, r, ntiles, blk, true, blk ? 0 : cfg.item, &listed, st))) return rc;
+    if (!blk && !listed) {
         k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, r.bcnt, nb, cfg.item, r.items, r.ctr + 2,
                                                       (int)plan_items_cap(ntiles, nb));
         idx->kernel_launches++;
@@ -2280,8 +2296,6 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
         if (timed)
             GTS_CUDA_TRY(cudaEventRecordWithFlags(idx->fev[1], st, capturing ? cudaEventRecordExternal : 0));
     }
-    k_add_stat<<<1, 1, 0, st>>>(idx->d_stats + 6, 1ull);
-    idx->kernel_launches++;
     // light recheck over every query, then the full one over those with more
     // than 128 candidates: a persistent grid, as many CTAs as fit on the SMs,
     // walking their list
@@ -2915,8 +2929,9 @@ int search_range_fast(gts_index *idx, const int *d_qids, int qnum, float r, int 
             GTS_CUDA_TRY(cudaMemsetAsync(rb.bq_fill, 0, sizeof(int) * nb, st));
         }
         k_fast_arec<<<ntiles, 128, 0, st>>>(idx->rows, dq, rb.order, n, idx->dim, fs, rb.arec, rb.qt);
-        if ((rc = prune_enqueue(idx, fs, bs, rb, ntiles, blk, st))) return rc;
-        if (!blk)
+        bool listed = false;
+        if ((rc = prune_enqueue(idx, fs, bs, rb, ntiles, blk, false, blk ? 0 : 16, &listed, st))) return rc;
+        if (!blk && !listed)
             k_items<<<(ntiles + 127) / 128, 128, 0, st>>>(ntiles, rb.bcnt, nb, 16, rb.items, rb.ctr + 2,
                                                           (int)plan_items_cap(ntiles, nb));
         GTS_CUDA_TRY(cudaGetLastError());

@@ -160,17 +160,22 @@ inline FastSummary fast_summary(unsigned char *recs, const FastShape &fs, int nb
     return s;
 }
 
-// The tiles' needed superblocks (mask words sb_mask[tile][nsbw]) and then
-// their needed blocks (blist[tile][..] in ascending order, counts in bcnt;
-// with bmask, each block's lanes and pairs per block in bq_cnt), on the
-// tensor cores (fast_prune.cu).  The block pass carves its items and result
-// words from `bufs`, prune_block_bufs(ntiles, nb, bmask != nullptr) bytes.
+// The tiles' needed superblocks (mask words sb_mask[tile][nsbw]; cleared
+// first when `clear`) and then their needed blocks (blist[tile][..] in
+// ascending order, counts in bcnt; with bmask, each block's lanes and pairs
+// per block in bq_cnt), on the tensor cores (fast_prune.cu).  n_items: a
+// zeroed counter of the block pass's items.  The block pass carves its items and result words from `bufs`,
+// prune_block_bufs(ntiles, nb, bmask != nullptr) bytes.  With fitems the
+// block lists also become the tile filter's work items of `item` blocks
+// (full ones from the front at fn_items[0], each tile's partial one from
+// the back of fitems_cap at fn_items[1]; both counters zeroed).
 int prune_superblocks(const unsigned char *arec, const FastShape &fs, const FastSummary &bs, int nsb, int ntiles,
-                      const int *r2_bits, uint32_t *sb_mask, int nsbw, int *status, cudaStream_t st);
+                      const int *r2_bits, uint32_t *sb_mask, int nsbw, bool clear, int *status, cudaStream_t st);
 size_t prune_block_bufs(int ntiles, int nb, bool lanes);
 int prune_blocks(const unsigned char *arec, const FastShape &fs, const FastSummary &bs, int nb, int ntiles,
-                 const int *r2_bits, const uint32_t *sb_mask, int nsbw, unsigned char *bufs, int *blist, int *bcnt,
-                 uint4 *bmask, int *bq_cnt, unsigned long long *stats, int *status, cudaStream_t st);
+                 const int *r2_bits, const uint32_t *sb_mask, int nsbw, unsigned char *bufs, int *n_items, int *blist,
+                 int *bcnt, uint4 *bmask, int *bq_cnt, int item, int2 *fitems, int *fn_items, int fitems_cap,
+                 unsigned long long *stats, int *status, cudaStream_t st);
 
 // Result of the order construction, in the index's scratch: positions of
 // the final order (perm: position -> object id), the blocks as position

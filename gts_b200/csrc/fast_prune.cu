@@ -412,9 +412,12 @@ __global__ void __launch_bounds__(256) k_prune_list(const int4 *__restrict__ ite
                                                     const uint32_t *__restrict__ plm, const int *__restrict__ tfirst,
                                                     const int *__restrict__ tcnt, int *__restrict__ blist,
                                                     int *__restrict__ bcnt, int nbcap, uint4 *__restrict__ bmask,
-                                                    int *__restrict__ bq_cnt, unsigned long long *stats)
+                                                    int *__restrict__ bq_cnt, int item, int2 *__restrict__ fitems,
+                                                    int *__restrict__ fn_items, int fitems_cap,
+                                                    unsigned long long *stats)
 {
     __shared__ int wsum[8];
+    __shared__ int fbase;
     __shared__ unsigned long long tested_s;
     const int tile = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int f = tfirst[tile], n = tcnt[tile];
@@ -465,10 +468,18 @@ __global__ void __launch_bounds__(256) k_prune_list(const int4 *__restrict__ ite
     }
     if (tested) atomicAdd(&tested_s, tested);
     __syncthreads();
+    const int cnt = min(base, nbcap);
+    // the tile filter's work items (as k_items makes them): the full ones
+    // from the front, the partial one from the back
+    const int full = fitems ? cnt / item : 0, rem = fitems ? cnt - full * item : 0;
     if (t == 0) {
-        bcnt[tile] = min(base, nbcap);
+        bcnt[tile] = cnt;
         if (stats && tested_s) atomicAdd(&stats[7], tested_s);
+        if (full > 0) fbase = atomicAdd(&fn_items[0], full);
+        if (rem > 0) fitems[fitems_cap - 1 - atomicAdd(&fn_items[1], 1)] = make_int2(tile, full * item);
     }
+    __syncthreads();
+    for (int i = t; i < full; i += blockDim.x) fitems[fbase + i] = make_int2(tile, i * item);
 }
 
 size_t prune_smem(const FastShape &fs)
@@ -507,7 +518,7 @@ static int prune_grid(int total)
 }
 
 int prune_superblocks(const unsigned char *arec, const FastShape &fs, const FastSummary &bs, int nsb, int ntiles,
-                      const int *r2_bits, uint32_t *sb_mask, int nsbw, int *status, cudaStream_t st)
+                      const int *r2_bits, uint32_t *sb_mask, int nsbw, bool clear, int *status, cudaStream_t st)
 {
     PruneArgs a{};
     a.arec = arec;
@@ -524,7 +535,7 @@ int prune_superblocks(const unsigned char *arec, const FastShape &fs, const Fast
     a.nsbw = nsbw;
     a.status = status;
     // the epilogue warps OR their balls into the mask words
-    GTS_CUDA_TRY(cudaMemsetAsync(sb_mask, 0, sizeof(uint32_t) * (size_t)ntiles * nsbw, st));
+    if (clear) GTS_CUDA_TRY(cudaMemsetAsync(sb_mask, 0, sizeof(uint32_t) * (size_t)ntiles * nsbw, st));
     const size_t smem = prune_smem(fs);
     GTS_CUDA_TRY(cudaFuncSetAttribute(k_prune<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_prune<false><<<prune_grid(ntiles * a.ngroups), kPThreads, smem, st>>>(a);
@@ -537,13 +548,13 @@ size_t prune_block_bufs(int ntiles, int nb, bool lanes)
     const size_t cap = prune_items_cap(ntiles, nb);
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     return al(sizeof(int4) * std::max(cap, (size_t)1)) + al(sizeof(uint32_t) * std::max(cap, (size_t)1)) +
-           al(2 * sizeof(int) * (size_t)ntiles) + al(8 * sizeof(int)) +
-           (lanes ? al(sizeof(uint32_t) * 4 * kPG * std::max(cap, (size_t)1)) : 0);
+           al(2 * sizeof(int) * (size_t)ntiles) + (lanes ? al(sizeof(uint32_t) * 4 * kPG * std::max(cap, (size_t)1)) : 0);
 }
 
 int prune_blocks(const unsigned char *arec, const FastShape &fs, const FastSummary &bs, int nb, int ntiles,
-                 const int *r2_bits, const uint32_t *sb_mask, int nsbw, unsigned char *bufs, int *blist, int *bcnt,
-                 uint4 *bmask, int *bq_cnt, unsigned long long *stats, int *status, cudaStream_t st)
+                 const int *r2_bits, const uint32_t *sb_mask, int nsbw, unsigned char *bufs, int *n_items, int *blist,
+                 int *bcnt, uint4 *bmask, int *bq_cnt, int item, int2 *fitems, int *fn_items, int fitems_cap,
+                 unsigned long long *stats, int *status, cudaStream_t st)
 {
     const int ngroups = (nb + kPG - 1) / kPG;
     const int items_cap = (int)prune_items_cap(ntiles, nb);
@@ -554,12 +565,10 @@ int prune_blocks(const unsigned char *arec, const FastShape &fs, const FastSumma
     uint32_t *pword = (uint32_t *)take(sizeof(uint32_t) * std::max(items_cap, 1));
     int *tfirst = (int *)take(2 * sizeof(int) * (size_t)ntiles);
     int *tcnt = tfirst + ntiles;
-    int *n_items = (int *)take(8 * sizeof(int));
     uint32_t *plm = bmask ? (uint32_t *)take(sizeof(uint32_t) * 4 * kPG * (size_t)std::max(items_cap, 1)) : nullptr;
     const size_t gsmem = sizeof(uint32_t) * (size_t)ngroups;
     if (gsmem > 48 * 1024)
         GTS_CUDA_TRY(cudaFuncSetAttribute(k_prune_items, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem));
-    GTS_CUDA_TRY(cudaMemsetAsync(n_items, 0, sizeof(int), st));
     k_prune_items<<<ntiles, 256, gsmem, st>>>(sb_mask, nsbw, bs.sb_b0, ngroups, items, pword, n_items, items_cap,
                                               tfirst, tcnt);
     GTS_CUDA_TRY(cudaGetLastError());
@@ -586,7 +595,8 @@ int prune_blocks(const unsigned char *arec, const FastShape &fs, const FastSumma
     // leaves CTAs without items at once
     k_prune<true><<<prune_grid(items_cap), kPThreads, smem, st>>>(a);
     GTS_CUDA_TRY(cudaGetLastError());
-    k_prune_list<<<ntiles, 256, 0, st>>>(items, pword, plm, tfirst, tcnt, blist, bcnt, nb, bmask, bq_cnt, stats);
+    k_prune_list<<<ntiles, 256, 0, st>>>(items, pword, plm, tfirst, tcnt, blist, bcnt, nb, bmask, bq_cnt, item,
+                                         fitems, fn_items, fitems_cap, stats);
     GTS_CUDA_TRY(cudaGetLastError());
     return GTS_OK;
 }
