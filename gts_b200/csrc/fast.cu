@@ -1777,6 +1777,77 @@ __global__ void k_fast_keys(const int *qids, int qnum, const int *pos_of, int *k
     }
 }
 
+// Query order of a filter run in one CTA (nb <= kOrderMaxNb): the queries
+// sorted by the block of their slot (keys), ties by query index -- the order
+// a stable sort gives.  A counting sort in shared memory: per-block counts,
+// their exclusive scan, a scatter through shared-memory cursors; then the
+// queries of each block (a few per block) put in index order by insertion
+// sort.  A block with more than kOrderSortMax queries keeps their arrival
+// order: the order only groups the queries into tiles, the answers do not
+// depend on it.
+constexpr int kOrderThreads = 1024;
+constexpr int kOrderMaxNb = 24576;   // 2 x 4 bytes per block of shared memory
+constexpr int kOrderSortMax = 64;
+__global__ void __launch_bounds__(kOrderThreads) k_fast_order(const int *__restrict__ keys, int qnum, int nb,
+                                                              int *__restrict__ order)
+{
+    extern __shared__ int osm[];
+    int *start = osm, *cur = osm + nb;
+    __shared__ int wsum[kOrderThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    for (int b = t; b < nb; b += kOrderThreads) cur[b] = 0;
+    __syncthreads();
+    for (int i = t; i < qnum; i += kOrderThreads) atomicAdd(&cur[keys[i]], 1);
+    __syncthreads();
+    // exclusive scan of the counts: thread t sums its contiguous range of
+    // blocks, the CTA scans the sums, each thread writes its range's starts
+    const int per = (nb + kOrderThreads - 1) / kOrderThreads;
+    const int b0 = min(nb, t * per), b1 = min(nb, b0 + per);
+    int local = 0;
+    for (int b = b0; b < b1; b++) local += cur[b];
+    int x = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int v = wsum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        wsum[lane] = v;
+    }
+    __syncthreads();
+    int run = (warp > 0 ? wsum[warp - 1] : 0) + x - local;
+    for (int b = b0; b < b1; b++) {
+        const int c = cur[b];
+        start[b] = run;
+        cur[b] = run;
+        run += c;
+    }
+    __syncthreads();
+    for (int i = t; i < qnum; i += kOrderThreads) order[atomicAdd(&cur[keys[i]], 1)] = i;
+    __syncthreads();   // the CTA's writes to order are visible to all its threads
+    for (int b = t; b < nb; b += kOrderThreads) {
+        const int s0 = start[b], s1 = cur[b];
+        if (s1 - s0 < 2 || s1 - s0 > kOrderSortMax) continue;
+        for (int p = s0 + 1; p < s1; p++) {
+            const int v = order[p];
+            int q = p - 1;
+            while (q >= s0 && order[q] > v) {
+                order[q + 1] = order[q];
+                q--;
+            }
+            order[q + 1] = v;
+        }
+    }
+}
+
 // The start of a kNN filter run in one launch.  Per query i: an empty
 // candidate list, the starting bound (carry, else FLT_MAX; with selfk, the
 // smaller of that and the seed table's bound for the k at column jk) and the
@@ -2203,12 +2274,19 @@ static int fast_run_enqueue(gts_index *idx, const RunBufs &r, const int *d_qids,
         k_fast_seed_tab<<<(qnum + 255) / 256, 256, 0, st>>>(d_qids, qnum, bs.pos, bs.selfk, jk, r.r2);
         idx->kernel_launches++;
     }
-    // block ids are below nb: sort only the bits they use
-    int key_bits = 1;
-    while (key_bits < 32 && (1ll << key_bits) < (long long)nb) key_bits++;
-    size_t cb = r.cub_bytes;
-    GTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(r.cub, cb, r.keys, r.skeys, r.vals, r.order, qnum, 0, key_bits,
-                                                 st));
+    if (nb <= kOrderMaxNb) {
+        const size_t osmem = 2 * sizeof(int) * (size_t)nb;
+        GTS_CUDA_TRY(cudaFuncSetAttribute(k_fast_order, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)osmem));
+        k_fast_order<<<1, kOrderThreads, osmem, st>>>(r.keys, qnum, nb, r.order);
+        idx->kernel_launches++;
+    } else {
+        // block ids are below nb: sort only the bits they use
+        int key_bits = 1;
+        while (key_bits < 32 && (1ll << key_bits) < (long long)nb) key_bits++;
+        size_t cb = r.cub_bytes;
+        GTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(r.cub, cb, r.keys, r.skeys, r.vals, r.order, qnum, 0, key_bits,
+                                                     st));
+    }
     const bool blk = cfg.blk && r.bmask && fast_blk_stages(fs) >= 2;
     if (blk) {
         GTS_CUDA_TRY(cudaMemsetAsync(r.bq_cnt, 0, sizeof(int) * nb, st));
