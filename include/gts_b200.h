@@ -234,7 +234,8 @@ int gts_knn_device(gts_index *idx, const int *d_qids, int qnum, int k, int form,
                    float *d_kth, int *d_ids, float *d_dists, void *stream);
 
 /* No counterpart in the reference.  gts_knn_device's GTS_FORM_FAST results
- * (the unseeded BF16 filter + exact recheck) without any device allocation:
+ * (the BF16 filter seeded from the index's seed table, without the learned
+ * radius, + exact recheck) without any device allocation:
  * scratch is a fixed 12 MiB file-scope device array per device, so at most
  * 512 queries per call (more -> GTS_ERR_INVALID), L2 only, dim <= 128,
  * 1 <= k <= 64.  The index must already hold its filter records (made by
