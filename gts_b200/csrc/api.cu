@@ -387,9 +387,6 @@ extern "C" void gts_index_free(gts_index *idx)
     if (idx->graph_stream) cudaStreamDestroy(idx->graph_stream);
     for (int i = 0; i < 2; i++)
         if (idx->graph_ev[i]) cudaEventDestroy(idx->graph_ev[i]);
-    if (idx->side_stream) cudaStreamDestroy(idx->side_stream);
-    for (int i = 0; i < 2; i++)
-        if (idx->side_ev[i]) cudaEventDestroy(idx->side_ev[i]);
     if (idx->mlp_P) cudaFree(idx->mlp_P);
     if (idx->mlp_norm) cudaFree(idx->mlp_norm);
     if (idx->mlp_piv) cudaFree(idx->mlp_piv);

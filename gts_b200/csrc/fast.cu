@@ -2102,10 +2102,6 @@ static int fast_prepare(gts_index *idx, cudaStream_t st)
     idx->fast_recs = recs;
     idx->fast_nb = nb;
     idx->fast_nsb = nsb;
-    if (!idx->side_stream) {
-        GTS_CUDA_TRY(cudaStreamCreateWithFlags(&idx->side_stream, cudaStreamNonBlocking));
-        for (int i = 0; i < 2; i++) GTS_CUDA_TRY(cudaEventCreateWithFlags(&idx->side_ev[i], cudaEventDisableTiming));
-    }
     idx->device_bytes += bytes;
     return GTS_OK;
 }

@@ -76,10 +76,6 @@ struct gts_index {
     bool use_graphs = true;
     long long graph_launches = 0;
     long long graph_clock = 0;
-    // second stream of the filter pass: the own-block seeds run on it while
-    // the query sort and tile operands run on the first (fast.cu)
-    cudaStream_t side_stream = nullptr;
-    cudaEvent_t side_ev[2] = {nullptr, nullptr};
 
     // learned kNN radius (mlp.cu): parameters, input standardisation,
     // feature pivots; valid for the tree it was trained on
