@@ -2494,7 +2494,8 @@ static size_t plan_book(int qnum, int k, unsigned char *base, Book *b)
 struct FastCall {
     unsigned char *region;
     size_t region_bytes;
-    Book book[3];   // stage 0: unseeded filter, 1: filter from the bound reached, 2: plain traversal
+    Book book[3];   // stage 0: filter on table seeds (no learned radius), 1: filter from the bound reached,
+                    // 2: plain traversal
 };
 
 void graph_invalidate(gts_index *idx)
