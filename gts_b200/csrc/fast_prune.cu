@@ -9,10 +9,11 @@
 // (BF16 hi + lo, the same tile record the filter reads) and the B operand
 // holds each centre as three BF16 rows hi + mid + lo (an exact split of the
 // FP32 centre, the layout of the centre rows in the filter's block records).
-// The epilogue sums the three columns of a ball and applies the filter's own
-// certified ball test (the skip test of k_fast_tile), so the blocks kept are
-// a superset of those the filter would not skip.  Up to a padded dimension
-// of 128 (kFResKp); wider indexes use the FP32 pruning kernels in fast.cu.
+// The epilogue sums the three columns of a ball and applies a certified ball
+// test that skips less than the filter's own (the skip test of
+// k_fast_tile), so the blocks kept are a superset of those the filter would
+// not skip.  Up to a padded dimension of 128 (kFResKp); wider indexes use
+// the FP32 pruning kernels in fast.cu.
 //
 // Centre operands: all superblocks (or blocks) in id order, 3 rows per ball,
 // in the K-major 128-byte swizzled layout of an operand of R = 3 * n32 rows
@@ -179,15 +180,14 @@ __device__ __forceinline__ bool prune_wait(uint64_t *bar, uint32_t parity, const
     return false;
 }
 
-
 // Persistent CTAs (one per SM), each over a contiguous range of (tile,
 // group) items (consecutive items mostly share the tile, whose operand then
 // stays in shared memory).  Item j of the CTA uses stage and accumulator
 // j % kPS.
-//   copy thread (warp 8): the groups' centre operands, up to kPS items ahead
+//   copy thread (warp 16): the groups' centre operands, up to kPS items ahead
 //     (a stage is refilled as soon as the epilogue of its previous item is
 //     done).
-//   MMA thread (warp 9): the tile's operand when the tile changes (after
+//   MMA thread (warp 17): the tile's operand when the tile changes (after
 //     every MMA reading the old one), and per item one 128 x 96 x kp MMA
 //     pair (query hi, then lo) into the item's accumulator.
 //   epilogue (sixteen warps; warp w reads TMEM lanes 32 (w % 4) .. + 31 and
